@@ -1,0 +1,374 @@
+// oracle/ref_shim/ref_runtime.cpp -- a CPU stand-in for the reference's GPU
+// runtime, so that the reference's own host module (Modules/FieldModules/
+// Lenia.cpp) and parameter bus (LifeCore/Params/ParameterBus.cpp) run
+// unmodified on the host and drive the CPU-compiled reference shaders.
+//
+// TEST INFRASTRUCTURE ONLY. Built into oracle/_ref/ from the reference tree by
+// oracle/Makefile; used by tests/golden/make_golden.py to produce fixtures, by
+// the oracle cross-check tests, and by bench.py's reference arm. Never linked
+// into the product.
+//
+// What is re-implemented here (declarations are the reference's own headers):
+//   ResourcePool  LifeCore/Metal/ResourcePool.h:50-88  -> CPU images
+//   CommandGraph  LifeCore/Metal/CommandGraph.h:63-107 -> runs each pass at once
+//   ComputePass   LifeCore/Metal/CommandGraph.h:24-61  -> records binds
+//   ColorMapPass  LifeCore/Render/ColorMapPass.h:67-  -> no-op (presentation)
+// The session API at the bottom mirrors SceneRunner's per-frame flow for one
+// Lenia module (LifeCore/Sim/SceneRunner.cpp:138-246): scene numeric params
+// become ParameterBus bases (LifeCore/Params/Scene.cpp:96-113), then
+// updateCPU(audio) and encode(ctx) once per frame.
+#include "LifeCore/Metal/CommandGraph.h"
+#include "LifeCore/Metal/ResourcePool.h"
+#include "LifeCore/Params/ParameterBus.h"
+#include "LifeCore/Render/ColorMapPass.h"
+#include "LifeCore/Sim/SimulationModule.h"
+#include "Modules/FieldModules/Lenia.h"
+
+#include "ref_kernels.h"
+
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+namespace life {
+
+namespace {
+
+uint32_t channelsOf(PixelFormat f) {
+    switch (f) {
+    case PixelFormat::R16F:
+    case PixelFormat::R32F: return 1;
+    case PixelFormat::RG16F:
+    case PixelFormat::RG32F: return 2;
+    default: return 4;
+    }
+}
+
+struct CpuTexture {
+    TextureDesc desc;
+    std::vector<double> store;
+    metal::CpuImage img;
+    std::vector<float> lastUpload;  // the most recent CPU upload, as floats
+};
+
+}  // namespace
+
+struct ResourcePool::Impl {
+    std::vector<std::unique_ptr<CpuTexture>> textures;
+    CpuTexture* get(TextureHandle h) {
+        if (!h.valid() || h.index > textures.size()) return nullptr;
+        return textures[h.index - 1].get();
+    }
+};
+
+ResourcePool::ResourcePool(MetalContext&) : impl_(std::make_unique<Impl>()) {}
+ResourcePool::~ResourcePool() = default;
+
+TextureHandle ResourcePool::createTexture(const TextureDesc& desc) {
+    auto t = std::make_unique<CpuTexture>();
+    t->desc = desc;
+    t->img.width = desc.width;
+    t->img.height = desc.height;
+    t->img.channels = channelsOf(desc.format);
+    t->store.assign(size_t(desc.width) * desc.height * t->img.channels, 0.0);
+    t->img.data = t->store.data();
+    impl_->textures.push_back(std::move(t));
+    TextureHandle h;
+    h.index = uint32_t(impl_->textures.size());
+    h.generation = 1;
+    return h;
+}
+
+bool ResourcePool::uploadTexture(TextureHandle h, const void* data, size_t bytesPerRow) {
+    CpuTexture* t = impl_->get(h);
+    if (!t) return false;
+    const uint32_t ch = t->img.channels;
+    if (bytesPerRow != size_t(t->img.width) * ch * sizeof(float)) return false;
+    const float* src = static_cast<const float*>(data);
+    const size_t n = size_t(t->img.width) * t->img.height * ch;
+    t->lastUpload.assign(src, src + n);
+    for (size_t i = 0; i < n; ++i) t->store[i] = double(src[i]);
+    return true;
+}
+
+struct CommandGraph::Impl {
+    ResourcePool* pool = nullptr;
+    std::vector<std::string> passLabels;
+    // When set, an init pass writes this field instead of running its kernel
+    // (used to start the reference from a caller-chosen initial state).
+    const std::vector<float>* initOverride = nullptr;
+    uint64_t passCount = 0;
+};
+
+CommandGraph::CommandGraph(MetalContext&, ResourcePool& pool, PipelineCache&)
+    : impl_(std::make_unique<Impl>()) {
+    impl_->pool = &pool;
+}
+CommandGraph::~CommandGraph() = default;
+
+void CommandGraph::copyTexture(TextureHandle src, TextureHandle dst) {
+    CpuTexture* s = impl_->pool->impl().get(src);
+    CpuTexture* d = impl_->pool->impl().get(dst);
+    if (!s || !d || s->store.size() != d->store.size()) {
+        std::fprintf(stderr, "[ref] copyTexture: bad handles\n");
+        std::abort();
+    }
+    d->store = s->store;
+    d->img.data = d->store.data();
+    impl_->passLabels.push_back("blit.copyTexture");
+    impl_->passCount++;
+}
+
+void CommandGraph::dispatch(ComputePass& pass, uint32_t gridW, uint32_t gridH, uint32_t) {
+    metal::CpuImage* tex[8] = {};
+    const void* bytes[4] = {};
+    size_t nbytes[4] = {};
+    CpuTexture* writeTarget = nullptr;
+    for (const auto& tb : pass.textures_) {
+        CpuTexture* t = impl_->pool->impl().get(tb.handle);
+        if (!t || tb.index < 0 || tb.index >= 8) {
+            std::fprintf(stderr, "[ref] pass %s: bad texture bind\n", pass.label_.c_str());
+            std::abort();
+        }
+        tex[tb.index] = &t->img;
+        if (tb.index == 0) writeTarget = t;
+    }
+    for (const auto& bb : pass.bytes_) {
+        if (bb.index < 0 || bb.index >= 4) std::abort();
+        bytes[bb.index] = bb.data.data();
+        nbytes[bb.index] = bb.data.size();
+    }
+    impl_->passLabels.push_back(pass.label_);
+    impl_->passCount++;
+    const bool isInit = pass.function_ == "leniaInit" || pass.function_ == "leniaStampInit";
+    if (isInit && impl_->initOverride && writeTarget) {
+        const auto& f = *impl_->initOverride;
+        if (f.size() != size_t(writeTarget->img.width) * writeTarget->img.height) std::abort();
+        for (size_t i = 0; i < f.size(); ++i) writeTarget->store[i] = double(f[i]);
+        return;
+    }
+    if (!ref_dispatch(pass.function_, tex, bytes, nbytes, gridW, gridH)) {
+        std::fprintf(stderr, "[ref] unknown pipeline %s\n", pass.function_.c_str());
+        std::abort();
+    }
+}
+
+ComputePass::ComputePass(CommandGraph& graph, std::string label)
+    : graph_(graph), label_(std::move(label)) {}
+ComputePass& ComputePass::pipeline(std::string functionName) {
+    function_ = std::move(functionName);
+    return *this;
+}
+ComputePass& ComputePass::read(int index, TextureHandle h) {
+    textures_.push_back({index, h});
+    return *this;
+}
+ComputePass& ComputePass::write(int index, TextureHandle h) {
+    textures_.push_back({index, h});
+    return *this;
+}
+ComputePass& ComputePass::bytes(int index, const void* data, size_t size) {
+    const auto* p = static_cast<const uint8_t*>(data);
+    bytes_.push_back({index, std::vector<uint8_t>(p, p + size)});
+    return *this;
+}
+void ComputePass::dispatch2D(uint32_t width, uint32_t height) {
+    graph_.dispatch(*this, width, height, 1);
+}
+
+// Presentation is out of scope for the oracle: the colour map is a no-op.
+void ColorMapPass::configure(const nlohmann::json&) {}
+void ColorMapPass::encode(CommandGraph&, const std::string&, TextureHandle, TextureHandle,
+                          uint32_t, uint32_t, float) {}
+void ColorMapPass::encodeScaled(CommandGraph&, const std::string&, TextureHandle, TextureHandle,
+                                uint32_t, uint32_t, uint32_t, uint32_t) {}
+
+}  // namespace life
+
+// ---------------------------------------------------------------------------
+// Session C API (ctypes-friendly).
+
+namespace {
+
+alignas(64) unsigned char g_dummyDevice[256];  // stands in for MetalContext/PipelineCache
+
+struct RefSession {
+    life::ResourcePool pool;
+    life::CommandGraph graph;
+    life::ParameterBus bus;
+    life::LeniaModule module;
+    life::SimulationContext ctx;
+    std::string instance;
+    std::vector<float> initOverride;
+    double lastEncodeSeconds = 0.0;
+
+    RefSession()
+        : pool(*reinterpret_cast<life::MetalContext*>(g_dummyDevice)),
+          graph(*reinterpret_cast<life::MetalContext*>(g_dummyDevice), pool,
+                *reinterpret_cast<life::PipelineCache*>(g_dummyDevice)) {}
+};
+
+life::CpuTexture* texOf(RefSession* s, life::TextureHandle h) {
+    return s->pool.impl().get(h);
+}
+
+}  // namespace
+
+extern "C" {
+
+// params_json: the module's scene "params" object. scene_w/h: scene resolution.
+void* ref_create(const char* params_json, uint32_t scene_w, uint32_t scene_h,
+                 const char* instance) {
+    nlohmann::json j;
+    try {
+        j = nlohmann::json::parse(params_json);
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "[ref] params JSON parse error: %s\n", e.what());
+        return nullptr;
+    }
+    auto* s = new RefSession();
+    s->instance = instance ? instance : "lenia0";
+    // Scene.cpp:96-113: numeric and boolean params become bus base values.
+    for (auto it = j.begin(); it != j.end(); ++it) {
+        if (it.value().is_number())
+            s->bus.setBase(s->instance + "." + it.key(), it.value().get<float>());
+        else if (it.value().is_boolean())
+            s->bus.setBase(s->instance + "." + it.key(), it.value().get<bool>() ? 1.0f : 0.0f);
+    }
+    s->module.configure(s->instance, j);
+    s->ctx.metal = nullptr;
+    s->ctx.resources = &s->pool;
+    s->ctx.params = &s->bus;
+    s->ctx.graph = &s->graph;
+    s->ctx.width = scene_w;
+    s->ctx.height = scene_h;
+    s->module.setup(s->ctx);
+    return s;
+}
+
+void ref_destroy(void* h) { delete static_cast<RefSession*>(h); }
+
+void ref_set_base(void* h, const char* key, float value) {
+    auto* s = static_cast<RefSession*>(h);
+    s->bus.setBase(s->instance + "." + key, value);
+}
+
+void ref_reset(void* h, uint32_t seed) { static_cast<RefSession*>(h)->module.reset(seed); }
+
+// Makes the next init pass write `field` (sim_w*sim_h floats) instead of the
+// noise/stamp kernel. NULL clears the override.
+void ref_set_init_field(void* h, const float* field, size_t n) {
+    auto* s = static_cast<RefSession*>(h);
+    if (field) {
+        s->initOverride.assign(field, field + n);
+        s->graph.impl().initOverride = &s->initOverride;
+    } else {
+        s->initOverride.clear();
+        s->graph.impl().initOverride = nullptr;
+    }
+}
+
+// One SceneRunner frame for this module: updateCPU(audio) then encode(ctx).
+void ref_encode(void* h, uint32_t frame_index, uint32_t substeps, uint32_t audio_frame_index) {
+    auto* s = static_cast<RefSession*>(h);
+    life::AudioFeatureState audio;
+    audio.frameIndex = audio_frame_index;
+    s->ctx.frameIndex = frame_index;
+    s->ctx.substeps = substeps;
+    s->module.updateCPU(audio);
+    auto t0 = std::chrono::steady_clock::now();
+    s->module.encode(s->ctx);
+    auto t1 = std::chrono::steady_clock::now();
+    s->lastEncodeSeconds = std::chrono::duration<double>(t1 - t0).count();
+}
+
+double ref_last_encode_seconds(void* h) { return static_cast<RefSession*>(h)->lastEncodeSeconds; }
+
+void ref_field_size(void* h, uint32_t* w, uint32_t* hh) {
+    auto* s = static_cast<RefSession*>(h);
+    life::CpuTexture* t = texOf(s, s->module.outputField());
+    *w = t ? t->img.width : 0;
+    *hh = t ? t->img.height : 0;
+}
+
+// Copies the current state field (channel 0) to out (sim_w*sim_h floats).
+int ref_get_field(void* h, float* out, size_t n) {
+    auto* s = static_cast<RefSession*>(h);
+    life::CpuTexture* t = texOf(s, s->module.outputField());
+    if (!t || n != size_t(t->img.width) * t->img.height) return -1;
+    for (size_t i = 0; i < n; ++i) out[i] = float(t->store[i * t->img.channels]);
+    return 0;
+}
+
+// Overwrites the current state field (channel 0).
+int ref_put_field(void* h, const float* in, size_t n) {
+    auto* s = static_cast<RefSession*>(h);
+    life::CpuTexture* t = texOf(s, s->module.outputField());
+    if (!t || n != size_t(t->img.width) * t->img.height) return -1;
+    for (size_t i = 0; i < n; ++i) t->store[i * t->img.channels] = double(in[i]);
+    return 0;
+}
+
+// Fetches the most recent CPU upload into the texture whose label ends with
+// `suffix` (e.g. ".kernel", ".kernelImageUpload"). Returns the element count
+// (0 if none); copies at most cap floats.
+size_t ref_get_upload(void* h, const char* suffix, float* out, size_t cap) {
+    auto* s = static_cast<RefSession*>(h);
+    const std::string suf(suffix);
+    for (auto& t : s->pool.impl().textures) {
+        const std::string& l = t->desc.label;
+        if (l.size() >= suf.size() && l.compare(l.size() - suf.size(), suf.size(), suf) == 0) {
+            size_t n = t->lastUpload.size();
+            if (out) std::memcpy(out, t->lastUpload.data(), std::min(n, cap) * sizeof(float));
+            return n;
+        }
+    }
+    return 0;
+}
+
+// Copies the full contents (all channels) of the texture whose label ends
+// with `suffix`. Returns the element count.
+size_t ref_get_texture(void* h, const char* suffix, double* out, size_t cap) {
+    auto* s = static_cast<RefSession*>(h);
+    const std::string suf(suffix);
+    for (auto& t : s->pool.impl().textures) {
+        const std::string& l = t->desc.label;
+        if (l.size() >= suf.size() && l.compare(l.size() - suf.size(), suf.size(), suf) == 0) {
+            size_t n = t->store.size();
+            if (out) std::memcpy(out, t->store.data(), std::min(n, cap) * sizeof(double));
+            return n;
+        }
+    }
+    return 0;
+}
+
+uint64_t ref_pass_count(void* h) { return static_cast<RefSession*>(h)->graph.impl().passCount; }
+
+// Writes the label of pass i (in issue order) into buf; returns its length.
+size_t ref_pass_label(void* h, uint64_t i, char* buf, size_t cap) {
+    auto* s = static_cast<RefSession*>(h);
+    const auto& v = s->graph.impl().passLabels;
+    if (i >= v.size()) return 0;
+    if (buf && cap) {
+        size_t n = std::min(cap - 1, v[i].size());
+        std::memcpy(buf, v[i].data(), n);
+        buf[n] = 0;
+    }
+    return v[i].size();
+}
+
+void ref_clear_pass_log(void* h) {
+    auto* s = static_cast<RefSession*>(h);
+    s->graph.impl().passLabels.clear();
+}
+
+uint32_t ref_pcg(uint32_t v) { return ref_pcg_hash(v); }
+float ref_rand(uint32_t px, uint32_t py, uint32_t tag, uint32_t seed) {
+    return ref_rand01(px, py, tag, seed);
+}
+
+}  // extern "C"
