@@ -1,0 +1,356 @@
+#!/usr/bin/env python
+"""Benchmark: Lenia Mpixel-steps/s on one 1920x1080 world, 3 kernels R=24.
+
+A step is one Lenia substep (multi-kernel FFT convolution, growth, Euler
+step, clip) of the ``fft3_1080p`` workload (life_simulation_b200/workloads.py:
+seeded uniform patches, exponential kernel core, growth mode 0). Units are
+pixels x steps; ``value`` is whole-job Mpixel-steps/s.
+
+* value: state resident in HBM; K steps, each bracketed by CUDA events on
+  the launching stream, with a 256 MiB write between steps to flush the
+  126 MB L2 (outside the events); time = sum of the step intervals, max over
+  ranks. Under torchrun every rank steps its own world (replicas, no
+  collective on the data path; weak scaling).
+* e2e: the same metric through the C ABI with host buffers: per step
+  lenia_upload (pinned host -> device), lenia_step, lenia_download (device ->
+  pinned host), timed by CUDA events on the context stream.
+* roofline: the dominant kernel's algorithmic bytes per launch (HBM-bound
+  figures of the spectral path, per pixel: column pass 4 + 2K + 4K, row
+  growth pass 4K + 4 + 4 + 4) over its mean event-timed launch duration,
+  against the measured copy bandwidth in MEASURED_PEAKS.json.
+* cpu_baseline: the reference's own Lenia module and kernels compiled for
+  the CPU (oracle/_ref), on a bounded row band of the same workload.
+* --impl reference: that CPU reference alone, as the reference arm.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Lenia Mpixel-steps/s (FFT, 3 kernels, 1080p)"
+UNIT = "Mpixel-steps/s"
+WORKLOAD = "fft3_1080p"
+FALLBACK_HBM_GBS = 6650.0
+# dram__bytes_read.sum + dram__bytes_write.sum per launch of the dominant
+# kernel from one ncu capture (profiles/), None until captured.
+NCU_TRAFFIC_BYTES = {}
+
+
+def parse_args():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--workload", default=WORKLOAD)
+    ap.add_argument("--e2e-steps", type=int, default=None)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    return ap.parse_args()
+
+
+def dist_env():
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled every 200 ms."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def stop(self):
+        if not self.proc:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        if not self.rows:
+            return None
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "", 1).isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "", 1).isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if "Active" in r[5 + i]})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(self.rows)}
+
+
+def cpu_baseline_reference(params, w, h, init, seconds, band=64):
+    """The compiled reference on a bounded row band; Mpixel-steps/s."""
+    from oracle.lenia_oracle import RefLenia
+    r = RefLenia(params, w, h)
+    r.reset(2)
+    r.set_initial_field(init)
+    r.set_row_window(0, band)
+    r.encode(0, 1)  # init + one sample step (warm-up)
+    steps, t0 = 0, time.perf_counter()
+    while True:
+        r.encode(1 + steps, 1)
+        steps += 1
+        el = time.perf_counter() - t0
+        if el >= seconds or steps >= 1000:
+            break
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    conv = "direct convolution with kernels[0] (the reference falls back from convMode fft at a " \
+           "non-power-of-two size, Lenia.cpp:245-269)"
+    return {"value": w * band * steps / el / 1e6, "unit": UNIT, "cores": cores, "kind": "reference",
+            "sample": f"rows 0..{band} of the {w}x{h} field, {steps} substeps in {el:.1f} s; {conv}"}
+
+
+def cpu_baseline_port(params, w, h, init, seconds):
+    """The oracle port (FP64, FFT convolution) when oracle/_ref is absent."""
+    from oracle.lenia_oracle import OracleLenia
+    o = OracleLenia(params, w, h, "f64")
+    o.reset(2)
+    o.set_initial_field(init)
+    o.encode(0, 1)
+    steps, t0 = 0, time.perf_counter()
+    while True:
+        o.encode(1 + steps, 1)
+        steps += 1
+        el = time.perf_counter() - t0
+        if el >= seconds or steps >= 100:
+            break
+    return {"value": w * h * steps / el / 1e6, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"full {w}x{h} field, {steps} substeps in {el:.1f} s (FP64 oracle)"}
+
+
+def cpu_baseline(params, w, h, init, seconds):
+    from oracle.lenia_oracle import RefLenia
+    if RefLenia.available():
+        return cpu_baseline_reference(params, w, h, init, seconds)
+    return cpu_baseline_port(params, w, h, init, seconds)
+
+
+def base_line(args, n, steps, warmup, w, h, params):
+    return {
+        "metric": METRIC, "unit": UNIT, "n_gpus": n, "steps": steps, "warmup": warmup,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded uniform patches, SplitMix64 seed 2)",
+        "config": {"workload": args.workload, "width": w, "height": h,
+                   "kernels": len(params.get("kernels", [])) or 1, "radius": params.get("radius"),
+                   "kernel_core": params.get("kernelCore", "gaussShell"),
+                   "growth_mode": params.get("growthMode"),
+                   "l2": "flushed between timed steps (256 MiB write)",
+                   "parallelism": f"replicas x{n}" if n > 1 else "single world"},
+    }
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    from life_simulation_b200 import workloads as wl
+    from oracle.lenia_oracle import RefLenia
+    params, w, h, init = wl.workload(args.workload)
+    line = base_line(args, args.gpus, args.steps, args.warmup, w, h, params)
+    line["impl"] = "reference"
+    if not RefLenia.available():
+        # The compiled reference is missing; the oracle port stands in.
+        cb = cpu_baseline_port(params, w, h, init, 10.0)
+        line.update(value=cb["value"], ms_per_step=w * h / cb["value"] / 1e3, cpu_baseline=cb)
+        line["e2e"] = {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+        print(json.dumps(line))
+        return 0
+    band = 32
+    r = RefLenia(params, w, h)
+    r.reset(2)
+    r.set_initial_field(init)
+    r.set_row_window(0, band)
+    r.encode(0, 1)
+    for i in range(args.warmup):
+        r.encode(1 + i, 1)
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        r.encode(1 + args.warmup + i, 1)
+    el = time.perf_counter() - t0
+    value = w * band * args.steps / el / 1e6
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    line.update(value=value, ms_per_step=el * 1e3 / args.steps)
+    line["cpu_baseline"] = {
+        "value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+        "sample": f"each step: rows 0..{band} of the {w}x{h} field (one substep); the reference "
+                  "falls back from convMode fft to direct convolution with kernels[0] at this "
+                  "non-power-of-two size (Lenia.cpp:245-269)"}
+    line["e2e"] = {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+    print(json.dumps(line))
+    return 0
+
+
+def run_b200(args):
+    import torch
+
+    rank, world, local = dist_env()
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    import life_simulation_b200 as lb
+    from life_simulation_b200 import workloads as wl
+
+    params, w, h, init = wl.workload(args.workload)
+    m = lb.LeniaModule(params, w, h)
+    m.reset(2 + rank)
+    m.upload(init)
+    stream = torch.cuda.current_stream()
+    sh = stream.cuda_stream
+    fp = m.frame_params(0)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+            torch.cuda.synchronize()
+
+    for i in range(max(3, args.warmup)):
+        fp.frame_index = fp.audio_frame = i
+        m.step(fp, 1, sh)
+    barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    m.profile(True)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for i in range(args.steps):
+        flush.zero_()
+        fp.frame_index = fp.audio_frame = args.warmup + i
+        evs[i][0].record(stream)
+        m.step(fp, 1, sh)
+        evs[i][1].record(stream)
+    barrier()
+    prof = m.profile_read()
+    m.profile(False)
+    cl = clocks.stop()
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    total_ms = float(sum(step_ms))
+    if world > 1:
+        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * w * h * args.steps / (total_ms / 1e3) / 1e6
+
+    # End to end through the C ABI with pinned host buffers.
+    e2e_steps = args.e2e_steps or max(10, args.steps // 4)
+    host_in = torch.empty((h, w), dtype=torch.float32, pin_memory=True).numpy()
+    host_out = torch.empty((h, w), dtype=torch.float32, pin_memory=True).numpy()
+    host_in[:] = m.field()
+    ctx_stream = torch.cuda.ExternalStream(m.stream())
+    barrier()
+    e2e_ms = 0.0
+    for i in range(e2e_steps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        fp.frame_index = fp.audio_frame = 100000 + i
+        a.record(ctx_stream)
+        m.upload(host_in)
+        m.step(fp, 1, None)
+        m.download_into(host_out)
+        b.record(ctx_stream)
+        b.synchronize()
+        e2e_ms += a.elapsed_time(b)
+        host_in, host_out = host_out, host_in
+    if world > 1:
+        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = world * w * h * e2e_steps / (e2e_ms / 1e3) / 1e6
+
+    # Roofline of the dominant kernel (HBM bound).
+    K = len(params.get("kernels", [])) or 1
+    bytes_px = {"column": 4 + 2 * K + 4 * K, "row_growth": 4 * K + 4 + 4 + 4, "row_fft": 4 + 4,
+                "direct": 8}
+    phases = {k: v for k, v in prof.items() if isinstance(v, dict) and v["count"] > 0}
+    dom = max(phases, key=lambda k: phases[k]["ms"])
+    launch_ms = phases[dom]["ms"] / phases[dom]["count"]
+    peak, peak_kind = measured_peaks()
+    achieved = bytes_px[dom] * w * h / (launch_ms / 1e3) / 1e9
+    step_bytes = (20 + 10 * K) * w * h  # canonical three-sweep bytes per pixel-step
+    mean_step_ms = total_ms / args.steps
+    line = base_line(args, world, args.steps, args.warmup, w, h, params)
+    line.update({
+        "value": value, "ms_per_step": mean_step_ms,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(w * h * 4),
+                "d2h_bytes_per_step": int(w * h * 4), "steps": e2e_steps},
+        "gpu_launches": int(prof["launches"]),
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                     "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": NCU_TRAFFIC_BYTES.get(dom),
+                     "algorithmic_bytes_per_launch": bytes_px[dom] * w * h,
+                     "launch_ms": launch_ms,
+                     "step": {"bytes": step_bytes, "achieved": step_bytes / (mean_step_ms / 1e3) / 1e9,
+                              "frac": step_bytes / (mean_step_ms / 1e3) / 1e9 / peak}},
+        "phases_ms_per_step": {k: v["ms"] / args.steps for k, v in phases.items()},
+        "clocks": cl,
+    })
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            line["cpu_baseline"] = cpu_baseline(params, w, h, init, args.cpu_seconds)
+        except Exception as e:  # the checker is optional; the GPU number stands
+            line["cpu_baseline"] = {"value": None, "error": str(e)}
+    if rank == 0:
+        print(json.dumps(line))
+    m.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_b200(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,229 @@
+/* include/lenia_b200.h -- C ABI of the B200 Lenia field update.
+ *
+ * A drop-in for the reference's Lenia module step (daitomanabe/life-simulation,
+ * Modules/FieldModules/Lenia.{h,cpp} behind the module plugin interface
+ * LifeCore/Sim/SimulationModule.h). Every entry point takes and returns plain
+ * C types; device memory is owned by the context (the reference's
+ * ResourcePool role, LifeCore/Metal/ResourcePool.h:1-6) and the caller sees
+ * device pointers only through lenia_field_device_ptr().
+ *
+ * All functions return a status: LENIA_OK (0); LENIA_WARN_FALLBACK (> 0) when
+ * the reference would have printed a "[life] ..." warning and fallen back
+ * (Lenia.cpp:226-228, :245-251, :259-269, :285-298, :306-312) -- the call
+ * succeeded and lenia_last_message() says what was substituted; or a negative
+ * LENIA_ERR_* code, after which the context is unchanged (or, for
+ * LENIA_ERR_CUDA, should be destroyed).
+ *
+ * Threading: a context is used from one host thread at a time (the
+ * reference's encode runs on the caller thread, LifeCore/Metal/
+ * CommandGraph.mm:69-88). Work is queued on the CUDA stream passed to
+ * lenia_encode()/lenia_step() (NULL = the context's own stream).
+ */
+#ifndef LENIA_B200_H
+#define LENIA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LENIA_B200_ABI_VERSION 1
+
+enum {
+    LENIA_OK = 0,
+    LENIA_WARN_FALLBACK = 1,
+    LENIA_ERR_INVALID_ARG = -1,
+    LENIA_ERR_UNSUPPORTED = -2,
+    LENIA_ERR_CUDA = -3,
+    LENIA_ERR_TIMEOUT = -4,
+    LENIA_ERR_STATE = -5,
+    LENIA_ERR_NO_DEVICE = -6,
+    LENIA_ERR_PARSE = -7,
+};
+
+/* Convolution paths. DIRECT and FFT are the reference's convMode values
+ * "direct" and "fft" (Lenia.cpp:213-214); DIRECT_MULTI ("directMulti") is
+ * this library's direct convolution over all "kernels" (the FFT path's math
+ * without the FFT), used to cross-check the two paths. */
+enum { LENIA_CONV_DIRECT = 0, LENIA_CONV_FFT = 1, LENIA_CONV_DIRECT_MULTI = 2 };
+/* Kernel radial profile. GAUSS_SHELL is the reference's (Lenia.cpp:410-446,
+ * :95-125); EXP is exp(4 - 1/(r(1-r))) (Chan's exponential core). */
+enum { LENIA_CORE_GAUSS_SHELL = 0, LENIA_CORE_EXP = 1 };
+enum { LENIA_INIT_NOISE = 0, LENIA_INIT_STAMP = 1 };
+
+/* One entry of the scene "kernels" array (KernelDef, Lenia.h:99-105). */
+typedef struct lenia_kernel_def {
+    float radius_scale; /* R_k = radius * radius_scale */
+    float mu;
+    float sigma;
+    float weight;       /* h_k */
+    uint32_t num_betas; /* 1..8 ring peaks */
+    float betas[8];
+} lenia_kernel_def;
+
+/* Setup-time parameters: the module's scene "params" block
+ * (Lenia.h:29-36, parsed at Lenia.cpp:208-357). */
+typedef struct lenia_config {
+    uint32_t sim_width;       /* 0 = scene width  (simWidth)  */
+    uint32_t sim_height;      /* 0 = scene height (simHeight) */
+    uint32_t conv_mode;       /* LENIA_CONV_* (convMode) */
+    uint32_t fft_any_size;    /* 0: the reference's power-of-two rule for FFT
+                                 (falls back to direct); 1: any even width and
+                                 a height whose factors are 2, 3, 5 */
+    uint32_t has_radius;      /* 0: radius defaults to 13 or the organism's R */
+    uint32_t radius;          /* radius (px) */
+    uint32_t num_kernels;     /* 0..4 entries of `kernels` (more: truncated) */
+    lenia_kernel_def kernels[4];
+    uint32_t kernel_core;     /* LENIA_CORE_* (kernelCore) */
+    float kernel_shell_mu;    /* kernelShellMu (0.5) */
+    float kernel_shell_sigma; /* kernelShellSigma (0.15) */
+    float init_coverage;      /* initCoverage (0.4) */
+    float init_scale;         /* initScale (24) */
+    uint32_t init_mode;       /* LENIA_INIT_* (initMode) */
+    /* Organism (initMode "stamp" / useOrganismParams, Lenia.cpp:271-321).
+     * organism_cells: row-major org_height x org_width values in [0,1], or
+     * NULL when no organism is given; the pointer is read during
+     * lenia_create only. */
+    const float* organism_cells;
+    uint32_t org_width, org_height;
+    float org_R, org_T, org_mu, org_sigma;
+    uint32_t stamp_count;          /* stampCount (6, max 32) */
+    uint32_t stamp_rotate;         /* stampRotate (1) */
+    uint32_t use_organism_params;  /* useOrganismParams (1) */
+} lenia_config;
+
+/* Per-frame values the reference reads through param(ctx, key, fallback)
+ * (Lenia.cpp:456-464) plus the frame's indices. */
+typedef struct lenia_frame_params {
+    float dt;
+    float growth_mu;
+    float growth_sigma;
+    float noise_amount;
+    float mu_jitter;
+    float inject_amount;
+    uint32_t inject_count;
+    uint32_t growth_mode;     /* 0 standard, 1 asymptotic */
+    uint32_t frame_index;     /* SimulationContext::frameIndex */
+    uint32_t audio_frame;     /* AudioUniforms::frameIndex */
+} lenia_frame_params;
+
+/* What setup resolved (after the reference's fallbacks). */
+typedef struct lenia_info {
+    uint32_t sim_width, sim_height;
+    uint32_t conv_mode;       /* path actually used */
+    uint32_t radius;          /* integer radius after rounding */
+    uint32_t num_kernels;     /* kernels convolved per substep */
+    uint32_t use_stamp_init;
+    uint64_t device_bytes;    /* device memory held by the context */
+    uint32_t fft_radix_row[8], fft_radix_col[8]; /* FFT plans (0-terminated) */
+} lenia_info;
+
+typedef struct lenia_ctx lenia_ctx;
+
+/* Fills `cfg` with the reference's defaults (Lenia.h:77-105). */
+void lenia_config_defaults(lenia_config* cfg);
+
+/* configure + setup (SimulationModule::configure, SimulationModule.h:112-115;
+ * LeniaModule::setup, Lenia.cpp:208-408) on the current CUDA device.
+ * scene_w/scene_h: SimulationContext::width/height. */
+int lenia_create(const lenia_config* cfg, uint32_t scene_w, uint32_t scene_h, lenia_ctx** out);
+
+/* Same, from the module's scene JSON "params" object, text as in the
+ * reference presets (Presets/lenia_*.json). Numeric and boolean leaves become
+ * per-frame base values (Scene::applyBaseParams, LifeCore/Params/Scene.cpp:
+ * 96-113). An "organism" path is read relative to the working directory or
+ * `base_dir` (may be NULL), as LeniaModule::setup does (Lenia.cpp:151-204). */
+int lenia_create_json(const char* params_json, uint32_t scene_w, uint32_t scene_h,
+                      const char* base_dir, lenia_ctx** out);
+
+int lenia_destroy(lenia_ctx* ctx);
+
+/* The host half of lenia_create_json without touching a device: what setup
+ * would resolve for these params (sizes, path after the reference's
+ * fallbacks, radius, kernel count); out->device_bytes is 0. Warnings are
+ * returned by lenia_last_message(NULL). Useful to validate a preset. */
+int lenia_inspect_json(const char* params_json, uint32_t scene_w, uint32_t scene_h,
+                       const char* base_dir, lenia_info* out);
+
+/* LeniaModule::reset (Lenia.cpp:448-451): seed = deriveSeed(seed, "LEN1");
+ * the next encode re-initialises the field. */
+int lenia_reset(lenia_ctx* ctx, uint32_t seed);
+
+/* Base value of a per-frame parameter, by the key param() uses ("dt",
+ * "growthMu", ...): ParameterBus::setBase for "<instance>.<key>"
+ * (LifeCore/Params/ParameterBus.h:98-99). */
+int lenia_set_param(lenia_ctx* ctx, const char* key, float value);
+/* Manual override layer (ParameterBus::setOverride / clearOverride,
+ * ParameterBus.h:111-113): wins over base and mappings. */
+int lenia_set_override(lenia_ctx* ctx, const char* key, float value);
+int lenia_clear_override(lenia_ctx* ctx, const char* key);
+/* The frame parameters encode would use now (param(ctx, key, fallback) for
+ * every key, Lenia.cpp:456-464), with the given frame indices. */
+int lenia_resolve_frame_params(lenia_ctx* ctx, uint32_t frame_index, uint32_t audio_frame,
+                               lenia_frame_params* out);
+
+/* One frame: LeniaModule::updateCPU + encode (Lenia.cpp:453-644). Runs the
+ * init pass if needed, then max(1, substeps) substeps with substep seeds
+ * pcgHash(seed ^ (frame_index*197 + s)). Parameters come from the base and
+ * override values above. Asynchronous on `stream` (NULL: context stream). */
+int lenia_encode(lenia_ctx* ctx, uint32_t frame_index, uint32_t substeps,
+                 uint32_t audio_frame, void* stream);
+
+/* Same as lenia_encode with explicit per-frame parameters (bypasses the
+ * parameter table). */
+int lenia_step(lenia_ctx* ctx, const lenia_frame_params* fp, uint32_t substeps, void* stream);
+
+/* Waits for the context's queued work; LENIA_ERR_CUDA if any failed
+ * (CommandGraph::lastFrameHadError, CommandGraph.h:89-94). */
+int lenia_sync(lenia_ctx* ctx);
+
+/* The state field (outputField / namedOutput("field"), Lenia.h:63-71):
+ * sim_height x sim_width floats, row-major. upload replaces it and marks
+ * the init as done (like SimulationModule::loadState, SimulationModule.h:
+ * 60-78); download waits for queued work. */
+int lenia_field_size(lenia_ctx* ctx, uint32_t* width, uint32_t* height);
+int lenia_upload(lenia_ctx* ctx, const float* host, size_t count);
+int lenia_download(lenia_ctx* ctx, float* host, size_t count);
+/* Device-to-device forms, ordered on `stream`. */
+int lenia_upload_device(lenia_ctx* ctx, const float* dev, size_t count, void* stream);
+int lenia_download_device(lenia_ctx* ctx, float* dev, size_t count, void* stream);
+/* Current device buffer of the field; valid until the next encode/step.
+ * Treat as read-only: write through lenia_upload_device. */
+int lenia_field_device_ptr(lenia_ctx* ctx, const float** dev);
+
+int lenia_get_info(lenia_ctx* ctx, lenia_info* out);
+
+/* The context's own CUDA stream (used when NULL is passed as `stream`). */
+int lenia_get_stream(lenia_ctx* ctx, void** stream);
+
+/* Per-pass GPU timing (the reference's per-pass counter samples,
+ * LifeCore/Metal/GPUTimer.h:1-40, CommandGraph.mm:108-122). With profiling
+ * on, every kernel launch is bracketed by CUDA events on its stream;
+ * lenia_profile_read waits for them and returns the accumulated device time
+ * and launch count per phase since profiling was enabled or last read.
+ * The launch counter runs whether or not profiling is on. */
+enum {
+    LENIA_PHASE_INIT = 0,       /* noise or stamp init */
+    LENIA_PHASE_DIRECT = 1,     /* fused direct convolution + growth */
+    LENIA_PHASE_ROW_FFT = 2,    /* row pass A -> row spectrum */
+    LENIA_PHASE_COLUMN = 3,     /* column FFT, spectrum products, inverse */
+    LENIA_PHASE_ROW_GROWTH = 4, /* inverse row pass + growth (+ next row FFT) */
+    LENIA_PHASE_COUNT = 8
+};
+typedef struct lenia_profile_data {
+    uint64_t launches;                  /* kernels launched since the last read */
+    uint32_t count[LENIA_PHASE_COUNT];  /* timed launches per phase */
+    double ms[LENIA_PHASE_COUNT];       /* device milliseconds per phase */
+} lenia_profile_data;
+int lenia_profile(lenia_ctx* ctx, int enable);
+int lenia_profile_read(lenia_ctx* ctx, lenia_profile_data* out);
+/* Message of the last warning or error on this context ("" if none). */
+const char* lenia_last_message(lenia_ctx* ctx);
+const char* lenia_status_string(int status);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LENIA_B200_H */

@@ -1,0 +1,363 @@
+"""B200-native Lenia field update -- Python binding of the C ABI.
+
+This package is a drop-in for the Lenia module step of LifeSimSuite
+(daitomanabe/life-simulation, ``Modules/FieldModules/Lenia.{h,cpp}`` behind
+``LifeCore/Sim/SimulationModule.h``). The compute path is the CUDA library
+``liblenia_b200.so`` built from ``csrc/`` for sm_100a; this module only binds
+its ``extern "C"`` entry points (``include/lenia_b200.h``) with ctypes and
+mirrors the reference module's lifecycle::
+
+    m = LeniaModule(params, scene_w, scene_h)   # configure + setup
+    m.reset(seed)                               # reset
+    m.encode(frame_index, substeps)             # updateCPU + encode
+    a = m.field()                               # outputField (download)
+
+There is no CPU fallback: importing the binding raises if the library is
+missing, and every call raises ``LeniaError`` on a failed status.
+"""
+from __future__ import annotations
+
+import ctypes
+import json
+import os
+from typing import Optional, Sequence
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "liblenia_b200.so")
+
+LENIA_OK = 0
+LENIA_WARN_FALLBACK = 1
+CONV_DIRECT, CONV_FFT, CONV_DIRECT_MULTI = 0, 1, 2
+CORE_GAUSS_SHELL, CORE_EXP = 0, 1
+INIT_NOISE, INIT_STAMP = 0, 1
+
+
+class LeniaError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"lenia status {status}: {message}")
+        self.status = status
+
+
+class KernelDef(ctypes.Structure):
+    """lenia_kernel_def (one entry of the scene "kernels" array)."""
+    _fields_ = [("radius_scale", ctypes.c_float), ("mu", ctypes.c_float),
+                ("sigma", ctypes.c_float), ("weight", ctypes.c_float),
+                ("num_betas", ctypes.c_uint32), ("betas", ctypes.c_float * 8)]
+
+
+class Config(ctypes.Structure):
+    """lenia_config (the scene "params" block, parsed)."""
+    _fields_ = [("sim_width", ctypes.c_uint32), ("sim_height", ctypes.c_uint32),
+                ("conv_mode", ctypes.c_uint32), ("fft_any_size", ctypes.c_uint32),
+                ("has_radius", ctypes.c_uint32), ("radius", ctypes.c_uint32),
+                ("num_kernels", ctypes.c_uint32), ("kernels", KernelDef * 4),
+                ("kernel_core", ctypes.c_uint32), ("kernel_shell_mu", ctypes.c_float),
+                ("kernel_shell_sigma", ctypes.c_float), ("init_coverage", ctypes.c_float),
+                ("init_scale", ctypes.c_float), ("init_mode", ctypes.c_uint32),
+                ("organism_cells", ctypes.POINTER(ctypes.c_float)),
+                ("org_width", ctypes.c_uint32), ("org_height", ctypes.c_uint32),
+                ("org_R", ctypes.c_float), ("org_T", ctypes.c_float),
+                ("org_mu", ctypes.c_float), ("org_sigma", ctypes.c_float),
+                ("stamp_count", ctypes.c_uint32), ("stamp_rotate", ctypes.c_uint32),
+                ("use_organism_params", ctypes.c_uint32)]
+
+
+class FrameParams(ctypes.Structure):
+    """lenia_frame_params (the per-frame param() values)."""
+    _fields_ = [("dt", ctypes.c_float), ("growth_mu", ctypes.c_float),
+                ("growth_sigma", ctypes.c_float), ("noise_amount", ctypes.c_float),
+                ("mu_jitter", ctypes.c_float), ("inject_amount", ctypes.c_float),
+                ("inject_count", ctypes.c_uint32), ("growth_mode", ctypes.c_uint32),
+                ("frame_index", ctypes.c_uint32), ("audio_frame", ctypes.c_uint32)]
+
+
+class Info(ctypes.Structure):
+    _fields_ = [("sim_width", ctypes.c_uint32), ("sim_height", ctypes.c_uint32),
+                ("conv_mode", ctypes.c_uint32), ("radius", ctypes.c_uint32),
+                ("num_kernels", ctypes.c_uint32), ("use_stamp_init", ctypes.c_uint32),
+                ("device_bytes", ctypes.c_uint64), ("fft_radix_row", ctypes.c_uint32 * 8),
+                ("fft_radix_col", ctypes.c_uint32 * 8)]
+
+
+# Every symbol include/lenia_b200.h declares (checked by the CPU tests).
+EXPORTS = (
+    "lenia_config_defaults", "lenia_create", "lenia_create_json", "lenia_inspect_json",
+    "lenia_destroy",
+    "lenia_reset", "lenia_set_param", "lenia_set_override", "lenia_clear_override",
+    "lenia_resolve_frame_params", "lenia_encode", "lenia_step", "lenia_sync",
+    "lenia_field_size", "lenia_upload", "lenia_download", "lenia_upload_device",
+    "lenia_download_device", "lenia_field_device_ptr", "lenia_get_info",
+    "lenia_get_stream", "lenia_profile", "lenia_profile_read",
+    "lenia_last_message", "lenia_status_string",
+)
+
+PHASES = ("init", "direct", "row_fft", "column", "row_growth")
+
+
+class ProfileData(ctypes.Structure):
+    _fields_ = [("launches", ctypes.c_uint64), ("count", ctypes.c_uint32 * 8),
+                ("ms", ctypes.c_double * 8)]
+
+_LIB = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Loads liblenia_b200.so (raises if it has not been built)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(path):
+        raise ImportError(f"{path} is missing: build it with `python -m life_simulation_b200.build`")
+    L = ctypes.CDLL(path)
+    P, u32, i32 = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int
+    pp = ctypes.POINTER(ctypes.c_void_p)
+    L.lenia_config_defaults.argtypes = [ctypes.POINTER(Config)]
+    L.lenia_config_defaults.restype = None
+    L.lenia_create.argtypes = [ctypes.POINTER(Config), u32, u32, pp]
+    L.lenia_create_json.argtypes = [ctypes.c_char_p, u32, u32, ctypes.c_char_p, pp]
+    L.lenia_inspect_json.argtypes = [ctypes.c_char_p, u32, u32, ctypes.c_char_p, ctypes.POINTER(Info)]
+    L.lenia_destroy.argtypes = [P]
+    L.lenia_reset.argtypes = [P, u32]
+    L.lenia_set_param.argtypes = [P, ctypes.c_char_p, ctypes.c_float]
+    L.lenia_set_override.argtypes = [P, ctypes.c_char_p, ctypes.c_float]
+    L.lenia_clear_override.argtypes = [P, ctypes.c_char_p]
+    L.lenia_resolve_frame_params.argtypes = [P, u32, u32, ctypes.POINTER(FrameParams)]
+    L.lenia_encode.argtypes = [P, u32, u32, u32, P]
+    L.lenia_step.argtypes = [P, ctypes.POINTER(FrameParams), u32, P]
+    L.lenia_sync.argtypes = [P]
+    L.lenia_field_size.argtypes = [P, ctypes.POINTER(u32), ctypes.POINTER(u32)]
+    L.lenia_upload.argtypes = [P, P, ctypes.c_size_t]
+    L.lenia_download.argtypes = [P, P, ctypes.c_size_t]
+    L.lenia_upload_device.argtypes = [P, P, ctypes.c_size_t, P]
+    L.lenia_download_device.argtypes = [P, P, ctypes.c_size_t, P]
+    L.lenia_field_device_ptr.argtypes = [P, pp]
+    L.lenia_get_info.argtypes = [P, ctypes.POINTER(Info)]
+    L.lenia_get_stream.argtypes = [P, pp]
+    L.lenia_profile.argtypes = [P, i32]
+    L.lenia_profile_read.argtypes = [P, ctypes.POINTER(ProfileData)]
+    L.lenia_last_message.argtypes = [P]
+    L.lenia_last_message.restype = ctypes.c_char_p
+    L.lenia_status_string.argtypes = [i32]
+    L.lenia_status_string.restype = ctypes.c_char_p
+    for name in EXPORTS:
+        getattr(L, name)  # raises AttributeError if the build lacks a symbol
+    _LIB = L
+    return L
+
+
+def default_config() -> Config:
+    c = Config()
+    load_library().lenia_config_defaults(ctypes.byref(c))
+    return c
+
+
+def config_from_params(params: dict) -> Config:
+    """A lenia_config from a scene ``params`` dict (organism given as cells)."""
+    c = default_config()
+    c.sim_width = int(params.get("simWidth", 0))
+    c.sim_height = int(params.get("simHeight", 0))
+    c.conv_mode = {"fft": CONV_FFT, "directMulti": CONV_DIRECT_MULTI}.get(params.get("convMode", "direct"), CONV_DIRECT)
+    c.fft_any_size = int(bool(params.get("fftAnySize", False)))
+    if "radius" in params:
+        c.has_radius, c.radius = 1, int(params["radius"])
+    ks = params.get("kernels") or []
+    c.num_kernels = len(ks)
+    for i, k in enumerate(ks[:4]):
+        b = list(k.get("betas") or [1.0])
+        c.kernels[i].radius_scale = k.get("radiusScale", 1.0)
+        c.kernels[i].mu = k.get("mu", 0.15)
+        c.kernels[i].sigma = k.get("sigma", 0.017)
+        c.kernels[i].weight = k.get("weight", 1.0)
+        c.kernels[i].num_betas = len(b)
+        for j, v in enumerate(b[:8]):
+            c.kernels[i].betas[j] = v
+    c.kernel_core = CORE_EXP if params.get("kernelCore", "gaussShell") == "exp" else CORE_GAUSS_SHELL
+    c.kernel_shell_mu = params.get("kernelShellMu", 0.5)
+    c.kernel_shell_sigma = params.get("kernelShellSigma", 0.15)
+    c.init_coverage = params.get("initCoverage", 0.4)
+    c.init_scale = params.get("initScale", 24.0)
+    c.init_mode = INIT_STAMP if params.get("initMode", "noise") == "stamp" else INIT_NOISE
+    c.stamp_count = min(32, int(params.get("stampCount", 6)))
+    c.stamp_rotate = int(bool(params.get("stampRotate", True)))
+    c.use_organism_params = int(bool(params.get("useOrganismParams", True)))
+    return c
+
+
+class LeniaModule:
+    """The reference LeniaModule's lifecycle over the CUDA library.
+
+    ``params``: the module's scene ``params`` dict (or its JSON text), exactly
+    as in the reference presets; ``scene_w``/``scene_h``: the scene size
+    (``SimulationContext::width/height``). ``base_dir`` resolves a relative
+    ``organism`` path. A setup fallback of the reference is not an error:
+    ``self.warning`` holds its message.
+    """
+
+    def __init__(self, params, scene_w: int, scene_h: int, base_dir: Optional[str] = None):
+        L = load_library()
+        self._L = L
+        self._h = ctypes.c_void_p()
+        text = params if isinstance(params, str) else json.dumps(params)
+        rc = L.lenia_create_json(text.encode(), scene_w, scene_h,
+                                 base_dir.encode() if base_dir else None, ctypes.byref(self._h))
+        if rc < 0:
+            raise LeniaError(rc, L.lenia_last_message(None).decode(errors="replace"))
+        self.warning = L.lenia_last_message(self._h).decode(errors="replace") if rc > 0 else ""
+        w, h = ctypes.c_uint32(), ctypes.c_uint32()
+        self._check(L.lenia_field_size(self._h, ctypes.byref(w), ctypes.byref(h)))
+        self.width, self.height = w.value, h.value
+
+    @classmethod
+    def from_config(cls, cfg: Config, scene_w: int, scene_h: int) -> "LeniaModule":
+        self = cls.__new__(cls)
+        L = load_library()
+        self._L = L
+        self._h = ctypes.c_void_p()
+        rc = L.lenia_create(ctypes.byref(cfg), scene_w, scene_h, ctypes.byref(self._h))
+        if rc < 0:
+            raise LeniaError(rc, L.lenia_last_message(None).decode(errors="replace"))
+        self.warning = L.lenia_last_message(self._h).decode(errors="replace") if rc > 0 else ""
+        w, h = ctypes.c_uint32(), ctypes.c_uint32()
+        self._check(L.lenia_field_size(self._h, ctypes.byref(w), ctypes.byref(h)))
+        self.width, self.height = w.value, h.value
+        return self
+
+    def _check(self, rc: int) -> int:
+        if rc < 0:
+            msg = self._L.lenia_last_message(self._h).decode(errors="replace")
+            raise LeniaError(rc, msg or self._L.lenia_status_string(rc).decode())
+        return rc
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            self._L.lenia_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def reset(self, seed: int) -> None:
+        self._check(self._L.lenia_reset(self._h, seed & 0xFFFFFFFF))
+
+    def set_param(self, key: str, value: float) -> None:
+        self._check(self._L.lenia_set_param(self._h, key.encode(), value))
+
+    def set_override(self, key: str, value: float) -> None:
+        self._check(self._L.lenia_set_override(self._h, key.encode(), value))
+
+    def clear_override(self, key: str) -> None:
+        self._check(self._L.lenia_clear_override(self._h, key.encode()))
+
+    def frame_params(self, frame_index: int = 0, audio_frame: Optional[int] = None) -> FrameParams:
+        fp = FrameParams()
+        af = frame_index if audio_frame is None else audio_frame
+        self._check(self._L.lenia_resolve_frame_params(self._h, frame_index, af, ctypes.byref(fp)))
+        return fp
+
+    def encode(self, frame_index: int, substeps: int = 1, audio_frame: Optional[int] = None,
+               stream: Optional[int] = None) -> None:
+        af = frame_index if audio_frame is None else audio_frame
+        self._check(self._L.lenia_encode(self._h, frame_index, substeps, af,
+                                         ctypes.c_void_p(stream) if stream else None))
+
+    def step(self, fp: FrameParams, substeps: int = 1, stream: Optional[int] = None) -> None:
+        self._check(self._L.lenia_step(self._h, ctypes.byref(fp), substeps,
+                                       ctypes.c_void_p(stream) if stream else None))
+
+    def sync(self) -> None:
+        self._check(self._L.lenia_sync(self._h))
+
+    def field(self) -> np.ndarray:
+        out = np.empty((self.height, self.width), np.float32)
+        self._check(self._L.lenia_download(self._h, out.ctypes.data_as(ctypes.c_void_p), out.size))
+        return out
+
+    def download_into(self, out: np.ndarray) -> np.ndarray:
+        """Downloads the field into a caller buffer (e.g. pinned memory)."""
+        if out.dtype != np.float32 or not out.flags.c_contiguous or out.size != self.width * self.height:
+            raise ValueError("out must be a contiguous float32 array of the field's size")
+        self._check(self._L.lenia_download(self._h, out.ctypes.data_as(ctypes.c_void_p), out.size))
+        return out
+
+    def upload(self, a: np.ndarray) -> None:
+        a = np.ascontiguousarray(a, np.float32)
+        if a.size != self.width * self.height:
+            raise ValueError("field size mismatch")
+        self._check(self._L.lenia_upload(self._h, a.ctypes.data_as(ctypes.c_void_p), a.size))
+
+    def upload_device(self, ptr: int, stream: Optional[int] = None) -> None:
+        self._check(self._L.lenia_upload_device(self._h, ctypes.c_void_p(ptr), self.width * self.height,
+                                                ctypes.c_void_p(stream) if stream else None))
+
+    def download_device(self, ptr: int, stream: Optional[int] = None) -> None:
+        self._check(self._L.lenia_download_device(self._h, ctypes.c_void_p(ptr), self.width * self.height,
+                                                  ctypes.c_void_p(stream) if stream else None))
+
+    def field_device_ptr(self) -> int:
+        p = ctypes.c_void_p()
+        self._check(self._L.lenia_field_device_ptr(self._h, ctypes.byref(p)))
+        return int(p.value or 0)
+
+    def stream(self) -> int:
+        """Handle of the context's own CUDA stream."""
+        p = ctypes.c_void_p()
+        self._check(self._L.lenia_get_stream(self._h, ctypes.byref(p)))
+        return int(p.value or 0)
+
+    def profile(self, enable: bool = True) -> None:
+        """Starts (or stops) per-launch CUDA-event timing; resets counters."""
+        self._check(self._L.lenia_profile(self._h, int(enable)))
+
+    def profile_read(self) -> dict:
+        """Device ms and launches per phase since the last read."""
+        d = ProfileData()
+        self._check(self._L.lenia_profile_read(self._h, ctypes.byref(d)))
+        out = {"launches": int(d.launches)}
+        for i, name in enumerate(PHASES):
+            out[name] = {"count": int(d.count[i]), "ms": float(d.ms[i])}
+        return out
+
+    def info(self) -> dict:
+        i = Info()
+        self._check(self._L.lenia_get_info(self._h, ctypes.byref(i)))
+        return {"sim_width": i.sim_width, "sim_height": i.sim_height, "conv_mode": i.conv_mode,
+                "radius": i.radius, "num_kernels": i.num_kernels, "use_stamp_init": i.use_stamp_init,
+                "device_bytes": i.device_bytes,
+                "fft_radix_row": [r for r in i.fft_radix_row if r],
+                "fft_radix_col": [r for r in i.fft_radix_col if r]}
+
+
+def inspect(params, scene_w: int, scene_h: int, base_dir: Optional[str] = None) -> dict:
+    """What setup would resolve for these params, without a device
+    (``lenia_inspect_json``): sizes, the path after the reference's
+    fallbacks, radius, kernel count, FFT plans, and ``warning``."""
+    L = load_library()
+    text = params if isinstance(params, str) else json.dumps(params)
+    i = Info()
+    rc = L.lenia_inspect_json(text.encode(), scene_w, scene_h,
+                              base_dir.encode() if base_dir else None, ctypes.byref(i))
+    msg = L.lenia_last_message(None).decode(errors="replace")
+    if rc < 0:
+        raise LeniaError(rc, msg)
+    return {"sim_width": i.sim_width, "sim_height": i.sim_height, "conv_mode": i.conv_mode,
+            "radius": i.radius, "num_kernels": i.num_kernels, "use_stamp_init": i.use_stamp_init,
+            "fft_radix_row": [r for r in i.fft_radix_row if r],
+            "fft_radix_col": [r for r in i.fft_radix_col if r],
+            "status": rc, "warning": msg if rc > 0 else ""}
+
+
+def make_frame_params(dt=0.1, growth_mu=0.15, growth_sigma=0.017, noise_amount=0.0, mu_jitter=0.0,
+                      inject_amount=0.0, inject_count=3, growth_mode=1, frame_index=0,
+                      audio_frame=None) -> FrameParams:
+    fp = FrameParams()
+    fp.dt, fp.growth_mu, fp.growth_sigma = dt, growth_mu, growth_sigma
+    fp.noise_amount, fp.mu_jitter, fp.inject_amount = noise_amount, mu_jitter, inject_amount
+    fp.inject_count, fp.growth_mode = inject_count, growth_mode
+    fp.frame_index = frame_index
+    fp.audio_frame = frame_index if audio_frame is None else audio_frame
+    return fp

@@ -1,0 +1,88 @@
+// life_simulation_b200/csrc/lenia_device.cuh -- device helpers shared by
+// every Lenia kernel: the PCG hash (bit-exact with the reference), and the
+// growth map + Euler step + noise + blob injection + clip epilogue.
+#pragma once
+#include <cstdint>
+
+#include "lenia_types.h"
+
+namespace lenia {
+
+// pcg_hash, Shaders/Common/Random.metal:5-9 (integer, bit-exact).
+__host__ __device__ __forceinline__ uint32_t pcg_hash(uint32_t v) {
+    uint32_t state = v * 747796405u + 2891336453u;
+    uint32_t word = ((state >> ((state >> 28u) + 4u)) ^ state) * 277803737u;
+    return (word >> 22u) ^ word;
+}
+
+// rand01, Shaders/Common/Random.metal:16-19: top 24 bits / 2^24, exact in f32.
+__host__ __device__ __forceinline__ float rand01(uint32_t px, uint32_t py, uint32_t tag,
+                                                 uint32_t seed) {
+    uint32_t h = pcg_hash(px ^ pcg_hash(py ^ pcg_hash(tag ^ seed)));
+    return float(h >> 8) * (1.0f / 16777216.0f);
+}
+
+// The per-pixel mu shift of muJitter (Lenia.metal:89-93 and :176-180).
+__device__ __forceinline__ float mu_jitter_shift(const StepParams& p, uint32_t gx, uint32_t gy) {
+    if (p.mu_jitter > 0.0f) {
+        float j = rand01(gx, gy, 401u + p.audio_frame % 613u, p.seed) - 0.5f;
+        return j * p.mu_jitter * 0.05f;
+    }
+    return 0.0f;
+}
+
+// bell(u; mu, sigma) = exp(-0.5 t^2), t = (u - mu) / sigma (Lenia.metal:156-159).
+__device__ __forceinline__ float bell(float u, float mu, float sigma) {
+    float t = (u - mu) / sigma;
+    return expf(-0.5f * t * t);
+}
+
+// Running growth sums over kernels in the reference's order
+// (Lenia.metal:188-195): sum_k h_k*bell_k and sum_k h_k*(2*bell_k - 1).
+struct GrowthAcc {
+    float weighted = 0.0f;
+    float std_sum = 0.0f;
+    __device__ __forceinline__ void add(float h, float b) {
+        weighted += h * b;
+        std_sum += h * (2.0f * b - 1.0f);
+    }
+};
+
+// Euler step, noise stir, blob injection and clip (Lenia.metal:197-231,
+// identical to leniaStep's :95-127 for one kernel of weight 1).
+__device__ __forceinline__ float growth_finish(const StepParams& p, float A, const GrowthAcc& acc,
+                                               uint32_t gx, uint32_t gy) {
+    float A2;
+    if (p.growth_mode == 1u) {
+        float target = (p.sum_weights > 1e-6f) ? (acc.weighted / p.sum_weights) : A;
+        A2 = A + p.dt * (target - A);
+    } else {
+        A2 = A + p.dt * acc.std_sum;
+    }
+    if (p.noise_amount > 0.0f) {
+        float n = rand01(gx, gy, 503u, p.seed) - 0.5f;
+        A2 += n * p.noise_amount * 0.03f;
+    }
+    if (p.inject_amount > 0.0f) {
+        float uvx = (float(gx) + 0.5f) / float(p.width);
+        float uvy = (float(gy) + 0.5f) / float(p.height);
+        float aspect = float(p.width) / float(p.height);
+        uint32_t cycle = p.frame_index / 12u;
+        float blobR = float(p.radius) * 0.9f / float(p.height);
+        for (uint32_t i = 0; i < p.inject_count; ++i) {
+            float cx = rand01(i, cycle, 811u, p.seed);
+            float cy = rand01(cycle, i, 823u, p.seed);
+            float dx = uvx - cx, dy = uvy - cy;
+            dx = dx - roundf(dx);
+            dy = dy - roundf(dy);
+            dx *= aspect;
+            float r2 = (dx * dx + dy * dy) / (blobR * blobR);
+            float bump = expf(-r2 * 0.5f);
+            float a = fminf(fmaxf(bump * p.inject_amount, 0.0f), 1.0f);
+            A2 = A2 + (0.6f - A2) * a;
+        }
+    }
+    return fminf(fmaxf(A2, 0.0f), 1.0f);
+}
+
+}  // namespace lenia

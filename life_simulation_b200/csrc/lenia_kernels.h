@@ -1,0 +1,73 @@
+// life_simulation_b200/csrc/lenia_kernels.h -- host-side launchers of the
+// CUDA kernels (internal interface between the module and the .cu files).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+#include "lenia_types.h"
+
+namespace lenia {
+
+// ----------------------------------------------------------------- direct
+enum DirectTileCfg { kDirectTile32x16 = 0, kDirectTile64x16 = 1, kDirectTile64x32 = 2 };
+
+struct DirectGeometry {
+    int r;      // halo radius (max kernel radius, integer)
+    int ksize;  // 2r + 1 kernel rows
+    int xp;     // r rounded up to a multiple of 4
+    int wp;     // weight row pitch = 2*xp + 8
+};
+
+size_t direct_smem_bytes(int tile_cfg, int nk, const DirectGeometry& g);
+cudaError_t launch_direct_step(int tile_cfg, int nk, const float* src, float* dst,
+                               const float* weights, const uint32_t* spans,
+                               const DirectGeometry& g, const StepParams& p, cudaStream_t stream);
+
+// -------------------------------------------------------------------- FFT
+constexpr int kMaxPasses = 8;
+
+// A mixed-radix plan for one transform length: n = prod(radix[0..npass)).
+struct FftPlan {
+    int n;
+    int npass;
+    int radix[kMaxPasses];
+};
+
+// Device geometry of the spectral path for a W x H field (W even).
+// Spectra are stored column-major: element (kx, ky) of a plane lives at
+// [kx * H + ky], kx in [0, M) with M = W/2; column 0 packs the real DC and
+// Nyquist columns as (re, im).
+struct FftGeometry {
+    int W, H, M;
+    FftPlan row;                 // length-M complex transform of a row
+    FftPlan col;                 // length-H complex transform of a column
+    const float2* tw_row;        // exp(-2 pi i t / M), t < M
+    const float2* tw_col;        // exp(-2 pi i t / H), t < H
+    const float2* tw_r2c;        // exp(-2 pi i k / W), k <= M
+    const float* khat;           // [nk][M + 1][H/2 + 1] real kernel spectra / (W*H)
+    int nk;
+    int rows_per_cta;            // rows per CTA in the row passes
+    int cols_per_cta;            // columns per CTA in the column pass
+};
+
+// Row pass: A (H x W) -> spectrum S (M x H column-major, packed column 0).
+cudaError_t launch_row_r2c(const FftGeometry& g, const float* A, float2* S, cudaStream_t s);
+// Column pass: S -> U_k = IFFT_H(FFT_H(S) * khat_k), k < nk (nk planes).
+cudaError_t launch_col_conv(const FftGeometry& g, const float2* S, float2* U, cudaStream_t s);
+// Row pass: U_k -> potentials -> growth -> A' (H x W); if S_next is not
+// null, also the row spectrum of A' (the next substep's first pass).
+cudaError_t launch_row_c2r_growth(const FftGeometry& g, const float2* U, const float* A,
+                                  float* A_out, float2* S_next, const StepParams& p,
+                                  cudaStream_t s);
+size_t fft_row_smem_bytes(const FftGeometry& g);
+size_t fft_col_smem_bytes(const FftGeometry& g);
+
+// ------------------------------------------------------------------ inits
+cudaError_t launch_init_noise(float* A, const InitParams& p, cudaStream_t s);
+cudaError_t launch_init_stamp(float* A, uint32_t w, uint32_t h, const float* org, uint32_t ow,
+                              uint32_t oh, uint32_t count, uint32_t rotate, uint32_t seed,
+                              cudaStream_t s);
+
+}  // namespace lenia

@@ -1,0 +1,227 @@
+// life_simulation_b200/csrc/lenia_module.h -- host-side mirror of the
+// reference's Lenia module (Modules/FieldModules/Lenia.h:50-196) on the
+// module lifecycle of LifeCore/Sim/SimulationModule.h:39-128
+// (configure -> setup -> reset -> per frame updateCPU + encode -> outputField),
+// driving the CUDA kernels of this library instead of Metal passes.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/lenia_b200.h"
+#include "json_lite.h"
+#include "lenia_kernels.h"
+#include "lenia_types.h"
+
+namespace lenia {
+
+// ParameterBus read contract used by param(ctx, key, fallback)
+// (LifeCore/Params/ParameterBus.cpp:345-355): the override wins, else
+// ((set ?: base) + sum of adds) * product of muls.
+class ParameterTable {
+public:
+    void setBase(const std::string& key, float v) { base_[key] = v; }
+    void setOverride(const std::string& key, float v) { override_[key] = v; }
+    void clearOverride(const std::string& key) { override_.erase(key); }
+    void setMapped(const std::string& key, float v) { set_[key] = v; }
+    void addMapped(const std::string& key, float v) { add_[key] += v; }
+    void mulMapped(const std::string& key, float v) {
+        auto it = mul_.find(key);
+        if (it == mul_.end()) mul_[key] = v;
+        else it->second *= v;
+    }
+    void clearMapped() {
+        set_.clear();
+        add_.clear();
+        mul_.clear();
+    }
+    float value(const std::string& key, float fallback) const;
+
+private:
+    std::map<std::string, float> base_, override_, set_, add_, mul_;
+};
+
+struct KernelDef {  // Lenia.h:99-105
+    float radius_scale = 1.0f;
+    float mu = 0.15f;
+    float sigma = 0.017f;
+    float weight = 1.0f;
+    std::vector<float> betas{1.0f};
+};
+
+struct OrganismData {  // Lenia.cpp:137-145
+    float R = 13.0f, T = 10.0f, mu = 0.15f, sigma = 0.015f;
+    uint32_t width = 0, height = 0;
+    std::vector<float> cells;
+};
+
+// Everything setup() reads, after parsing (C struct or JSON).
+struct ModuleConfig {
+    uint32_t sim_width = 0, sim_height = 0;
+    uint32_t conv_mode = LENIA_CONV_DIRECT;
+    bool fft_any_size = false;
+    bool has_radius = false;
+    uint32_t radius = 13;
+    bool has_kernels = false;
+    std::vector<KernelDef> kernels;
+    uint32_t kernel_core = LENIA_CORE_GAUSS_SHELL;
+    float shell_mu = 0.5f, shell_sigma = 0.15f;
+    float init_coverage = 0.4f, init_scale = 24.0f;
+    bool want_stamp = false;
+    bool has_organism_path = false;  // "organism" named (loaded or not)
+    bool organism_loaded = false;
+    OrganismData organism;
+    std::string organism_error;
+    uint32_t stamp_count = 6;
+    bool stamp_rotate = true;
+    bool use_organism_params = true;
+    std::vector<std::string> warnings;  // produced while parsing
+};
+
+class LeniaModule {
+public:
+    LeniaModule();
+    ~LeniaModule();
+    LeniaModule(const LeniaModule&) = delete;
+    LeniaModule& operator=(const LeniaModule&) = delete;
+
+    // SimulationModule::configure (SimulationModule.h:112-115).
+    void configure(std::string instance, ModuleConfig cfg) {
+        instance_ = std::move(instance);
+        cfg_ = std::move(cfg);
+    }
+    // LeniaModule::setup (Lenia.cpp:208-408). Returns LENIA_OK,
+    // LENIA_WARN_FALLBACK, or an error.
+    int setup(uint32_t scene_w, uint32_t scene_h);
+    // The host half of setup (sizes, paths, fallbacks, radius) without any
+    // device work; setup() calls it first.
+    int resolve(uint32_t scene_w, uint32_t scene_h);
+    // LeniaModule::reset (Lenia.cpp:448-451).
+    void reset(uint32_t seed);
+    // LeniaModule::updateCPU (Lenia.cpp:453): only the frame index of the
+    // audio state reaches the kernels (AudioUniforms::frameIndex).
+    void updateCPU(uint32_t audio_frame) { audio_frame_ = audio_frame; }
+    // LeniaModule::encode (Lenia.cpp:455-644) with per-frame values read
+    // from `params` (param(ctx, key, fallback)).
+    int encode(uint32_t frame_index, uint32_t substeps, const ParameterTable& params,
+               cudaStream_t stream);
+    // encode with explicit per-frame values.
+    int step(const lenia_frame_params& fp, uint32_t substeps, cudaStream_t stream);
+    // Per-frame values as encode would read them (Lenia.cpp:456-464).
+    lenia_frame_params resolveFrameParams(const ParameterTable& params, uint32_t frame_index,
+                                          uint32_t audio_frame) const;
+
+    // outputField (Lenia.h:63): the current state buffer on the device.
+    const float* outputField() const { return field_[cur_]; }
+    float* mutableField() { return field_[cur_]; }
+    void fieldWritten() {
+        needs_field_init_ = false;
+        spectrum_valid_ = false;
+    }
+    uint32_t width() const { return w_; }
+    uint32_t height() const { return h_; }
+    void info(lenia_info* out) const;
+    const std::string& message() const { return message_; }
+    void setMessage(std::string m) { message_ = std::move(m); }
+    cudaStream_t stream() const { return stream_; }
+
+    // Per-launch event timing (GPUTimer's role, LifeCore/Metal/GPUTimer.h).
+    void setProfiling(bool on);
+    int readProfile(lenia_profile_data* out);
+
+private:
+    // Launches `fn` as one kernel of `phase`, counted and, when profiling,
+    // bracketed by CUDA events on stream `s`.
+    template <typename F>
+    cudaError_t launch(int phase, cudaStream_t s, F&& fn);
+    cudaEvent_t takeEvent();
+    int fail(int code, const std::string& what);
+    int cudaFail(cudaError_t e, const char* where);
+    int buildDirectTables();
+    int buildSpectralTables(const std::vector<KernelDef>& eff);
+    int initField(const lenia_frame_params& fp, cudaStream_t s);
+    int initKernels(const lenia_frame_params& fp);
+    void fillStepParams(const lenia_frame_params& fp, uint32_t seed, StepParams& p) const;
+    void release();
+
+    std::string instance_ = "lenia0";
+    ModuleConfig cfg_;
+    std::string message_;
+    std::vector<std::string> warnings_;
+
+    // Resolved at setup.
+    uint32_t w_ = 0, h_ = 0;
+    bool use_fft_ = false, direct_multi_ = false, use_stamp_ = false;
+    uint32_t radius_ = 13;
+    float fallback_mu_ = 0.15f, fallback_sigma_ = 0.017f, fallback_dt_ = 0.1f;
+    std::vector<KernelDef> kernels_;
+    std::vector<float> direct_lut_;  // reference LUT, direct mode
+
+    // Runtime state.
+    uint32_t seed_ = 0;
+    uint32_t audio_frame_ = 0;
+    bool needs_field_init_ = true;
+    bool needs_kernel_init_ = true;
+    bool spectrum_valid_ = false;
+    int cur_ = 0;
+    int device_ = 0;
+    cudaStream_t stream_ = nullptr;
+
+    // Multi-kernel growth parameters fixed at init (Lenia.cpp:503-545).
+    uint32_t num_k_ = 1;
+    float k_mu_[kMaxKernels] = {0.15f, 0.15f, 0.15f, 0.15f};
+    float k_sigma_[kMaxKernels] = {0.017f, 0.017f, 0.017f, 0.017f};
+    float k_weight_[kMaxKernels] = {1.0f, 0.0f, 0.0f, 0.0f};
+
+    // Device resources.
+    float* field_[2] = {nullptr, nullptr};
+    float* d_weights_ = nullptr;
+    uint32_t* d_spans_ = nullptr;
+    float* d_org_ = nullptr;
+    float2* d_S_ = nullptr;
+    float2* d_U_ = nullptr;
+    float* d_khat_ = nullptr;
+    float2* d_tw_row_ = nullptr;
+    float2* d_tw_col_ = nullptr;
+    float2* d_tw_r2c_ = nullptr;
+    uint64_t device_bytes_ = 0;
+    DirectGeometry dgeo_{};
+    int direct_tile_ = kDirectTile64x16;
+    int direct_nk_ = 1;
+    FftGeometry fgeo_{};
+
+    // Launch accounting and profiling.
+    uint64_t launches_ = 0;
+    bool profiling_ = false;
+    struct TimedLaunch {
+        int phase;
+        cudaEvent_t start, stop;
+    };
+    std::vector<TimedLaunch> timed_;
+    std::vector<cudaEvent_t> event_pool_;
+};
+
+// Parsing of the scene "params" object (Lenia.cpp:208-357) and of the C
+// struct into ModuleConfig.
+int config_from_json(const Json& params, const std::string& base_dir, ModuleConfig& out,
+                     std::string& error);
+int config_from_struct(const lenia_config& c, ModuleConfig& out, std::string& error);
+
+// Host-side kernel construction shared with the batched form.
+void build_direct_lut(uint32_t radius, float shell_mu, float shell_sigma, uint32_t core,
+                      std::vector<float>& out);
+void build_ring_image(uint32_t w, uint32_t h, float radius_k, float shell_sigma,
+                      const std::vector<float>& betas, uint32_t core, std::vector<float>& out);
+bool fft_plan(int n, FftPlan& plan);
+void fill_twiddles(int n, std::vector<float2>& tw);
+// Real even spectrum of a wrap-centred kernel image, divided by (w*h):
+// out[kx * (h/2+1) + ky], kx <= w/2, ky <= h/2 (FP64, rounded once).
+void kernel_spectrum(const std::vector<float>& img, uint32_t w, uint32_t h,
+                     std::vector<float>& out);
+uint32_t pcg_hash_host(uint32_t v);
+uint32_t derive_seed(uint32_t global_seed, uint32_t tag);
+
+}  // namespace lenia

@@ -475,6 +475,7 @@ class RefLenia:
             L.ref_put_field.argtypes = [P, P, ctypes.c_size_t]
             L.ref_get_upload.restype = ctypes.c_size_t
             L.ref_get_upload.argtypes = [P, ctypes.c_char_p, P, ctypes.c_size_t]
+            L.ref_set_row_window.argtypes = [P, u32, u32]
             L.ref_pass_count.restype = ctypes.c_uint64
             L.ref_pass_count.argtypes = [P]
             L.ref_pcg.restype = u32
@@ -539,6 +540,10 @@ class RefLenia:
         if n:
             self.lib().ref_get_upload(self.h_, suffix.encode(), _ptr(out), n)
         return out
+
+    def set_row_window(self, y0: int, y1: int) -> None:
+        """Only rows [y0, y1) of the update passes run (y1 = 0: all rows)."""
+        self.lib().ref_set_row_window(self.h_, y0, y1)
 
     def pass_count(self) -> int:
         return int(self.lib().ref_pass_count(self.h_))

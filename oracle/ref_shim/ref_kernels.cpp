@@ -40,10 +40,15 @@ using metal::CpuImage;
 using RTex = metal::texture2d<float, access::read>;
 using WTex = metal::texture2d<float, access::write>;
 
+// Rows [g_y0, g_y1) of the grid run (the whole grid unless a row window is
+// set for a bounded timing sample).
+thread_local uint g_y0 = 0, g_y1 = ~0u;
+
 template <typename F>
 void grid2D(uint w, uint h, F&& f) {
+    const long y0 = long(g_y0), y1 = long(std::min(h, g_y1));
 #pragma omp parallel for schedule(static)
-    for (long y = 0; y < long(h); ++y)
+    for (long y = y0; y < y1; ++y)
         for (uint x = 0; x < w; ++x) f(uint2(x, uint(y)));
 }
 
@@ -65,8 +70,10 @@ float ref_rand01(uint32_t px, uint32_t py, uint32_t tag, uint32_t seed) {
 }
 
 bool ref_dispatch(const std::string& fn, CpuImage* const* tex, const void* const* bytes,
-                  const size_t* nbytes, uint32_t w, uint32_t h) {
+                  const size_t* nbytes, uint32_t w, uint32_t h, uint32_t y0, uint32_t y1) {
     using namespace refmsl;
+    g_y0 = y0;
+    g_y1 = y1;
     if (fn == "leniaInit") {
         const auto& p = as<LeniaParams>(bytes[0], nbytes[0], "LeniaParams");
         WTex dst(tex[0]);

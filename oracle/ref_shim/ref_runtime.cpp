@@ -102,6 +102,9 @@ struct CommandGraph::Impl {
     // (used to start the reference from a caller-chosen initial state).
     const std::vector<float>* initOverride = nullptr;
     uint64_t passCount = 0;
+    // Row window for the per-pixel update passes (leniaStep,
+    // leniaGrowthMulti): a bounded sample of a step for CPU timing.
+    uint32_t rowLo = 0, rowHi = ~0u;
 };
 
 CommandGraph::CommandGraph(MetalContext&, ResourcePool& pool, PipelineCache&)
@@ -151,7 +154,9 @@ void CommandGraph::dispatch(ComputePass& pass, uint32_t gridW, uint32_t gridH, u
         for (size_t i = 0; i < f.size(); ++i) writeTarget->store[i] = double(f[i]);
         return;
     }
-    if (!ref_dispatch(pass.function_, tex, bytes, nbytes, gridW, gridH)) {
+    const bool windowed = pass.function_ == "leniaStep" || pass.function_ == "leniaGrowthMulti";
+    const uint32_t y0 = windowed ? impl_->rowLo : 0u, y1 = windowed ? impl_->rowHi : ~0u;
+    if (!ref_dispatch(pass.function_, tex, bytes, nbytes, gridW, gridH, y0, y1)) {
         std::fprintf(stderr, "[ref] unknown pipeline %s\n", pass.function_.c_str());
         std::abort();
     }
@@ -344,6 +349,14 @@ size_t ref_get_texture(void* h, const char* suffix, double* out, size_t cap) {
         }
     }
     return 0;
+}
+
+// Restricts the per-pixel update passes to rows [y0, y1) (a bounded timing
+// sample of a step; rows outside keep their old values). y1 = 0: no window.
+void ref_set_row_window(void* h, uint32_t y0, uint32_t y1) {
+    auto* s = static_cast<RefSession*>(h);
+    s->graph.impl().rowLo = y1 ? y0 : 0u;
+    s->graph.impl().rowHi = y1 ? y1 : ~0u;
 }
 
 uint64_t ref_pass_count(void* h) { return static_cast<RefSession*>(h)->graph.impl().passCount; }

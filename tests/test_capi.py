@@ -1,0 +1,119 @@
+"""The C ABI library on the CPU: it loads, exports every entry point that
+include/lenia_b200.h declares, and its host logic (parameter parsing and
+the reference's setup fallbacks) resolves like the reference. No compute
+call needs a device here."""
+import json
+import os
+import re
+import subprocess
+
+import pytest
+
+import life_simulation_b200 as lb
+from tests.conftest import ROOT
+
+HEADER = os.path.join(ROOT, "include", "lenia_b200.h")
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(lenia_[a-z_0-9]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    lb.load_library()
+    out = subprocess.run(["nm", "-D", "--defined-only", lb.LIB_PATH], capture_output=True, text=True,
+                         check=True).stdout
+    exported = set(re.findall(r" T (lenia_\w+)", out))
+    decl = declared_functions()
+    assert decl, "no declarations parsed"
+    missing = [f for f in decl if f not in exported]
+    assert not missing, missing
+    assert set(decl) == set(lb.EXPORTS)
+
+
+def test_header_compiles_as_c():
+    r = subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-fsyntax-only", "-x", "c", HEADER],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+
+
+def test_status_strings():
+    L = lb.load_library()
+    assert L.lenia_status_string(0) == b"ok"
+    assert b"CUDA" in L.lenia_status_string(-3)
+
+
+def preset(name):
+    p = os.path.join("/root/reference/Presets", name)
+    if not os.path.exists(p):
+        pytest.skip("reference presets not present")
+    return json.load(open(p))["modules"][0]["params"]
+
+
+def test_inspect_direct_default():
+    r = lb.inspect({"radius": 13}, 256, 256)
+    assert r["conv_mode"] == lb.CONV_DIRECT and r["radius"] == 13 and r["status"] == 0
+
+
+def test_inspect_fft_pow2_rule_falls_back_like_reference():
+    p = {"convMode": "fft", "simWidth": 1920, "simHeight": 1080, "radius": 24,
+         "kernels": [{"betas": [1.0], "radiusScale": 0.5}]}
+    r = lb.inspect(p, 1280, 720)
+    assert r["status"] == lb.LENIA_WARN_FALLBACK
+    assert r["conv_mode"] == lb.CONV_DIRECT
+    assert r["radius"] == 12  # round(24 * kernels[0].radiusScale)
+    assert "powers of two" in r["warning"] and "kernels[0]" in r["warning"]
+
+
+def test_inspect_fft_any_size_mixed_radix():
+    p = {"convMode": "fft", "fftAnySize": True, "simWidth": 1920, "simHeight": 1080, "radius": 24,
+         "kernels": [{"betas": [1.0]}] * 3}
+    r = lb.inspect(p, 1920, 1080)
+    assert r["status"] == 0 and r["conv_mode"] == lb.CONV_FFT and r["num_kernels"] == 3
+    prod = lambda xs: eval("*".join(map(str, xs)))
+    assert prod(r["fft_radix_row"]) == 960 and prod(r["fft_radix_col"]) == 1080
+
+
+def test_inspect_unsupported_fft_size_falls_back():
+    p = {"convMode": "fft", "fftAnySize": True, "simWidth": 98, "simHeight": 70, "radius": 5}
+    r = lb.inspect(p, 98, 70)  # 49 = 7^2 has no 2/3/5 plan
+    assert r["conv_mode"] == lb.CONV_DIRECT and r["status"] == lb.LENIA_WARN_FALLBACK
+
+
+def test_inspect_kernels_truncated_to_four():
+    p = {"convMode": "fft", "simWidth": 64, "simHeight": 64, "kernels": [{"betas": [1.0]}] * 6}
+    r = lb.inspect(p, 64, 64)
+    assert r["num_kernels"] == 4 and "truncating" in r["warning"]
+
+
+def test_inspect_stamp_without_organism_falls_back():
+    r = lb.inspect({"initMode": "stamp"}, 64, 64)
+    assert r["use_stamp_init"] == 0 and "organism" in r["warning"]
+
+
+def test_inspect_organism_params(tmp_path):
+    org = tmp_path / "o.json"
+    org.write_text(json.dumps({"R": 11.5, "T": 4, "mu": 0.2, "sigma": 0.03, "cells": [[0.5, 1.0], [0.0, 0.25]]}))
+    r = lb.inspect({"initMode": "stamp", "organism": str(org)}, 64, 64)
+    assert r["use_stamp_init"] == 1 and r["radius"] == 12 and r["status"] == 0
+    bad = tmp_path / "bad.json"
+    bad.write_text(json.dumps({"cells": [[0.5, 1.5]]}))
+    r = lb.inspect({"initMode": "stamp", "organism": str(bad)}, 64, 64)
+    assert r["use_stamp_init"] == 0 and "out of [0,1]" in r["warning"]
+
+
+def test_inspect_reference_presets():
+    r = lb.inspect(preset("lenia_multikernel.json"), 1280, 720)
+    assert (r["sim_width"], r["sim_height"], r["conv_mode"], r["num_kernels"], r["radius"]) == (
+        1024, 512, lb.CONV_FFT, 3, 24)
+    r = lb.inspect(preset("lenia_basic.json"), 768, 768)
+    assert (r["conv_mode"], r["radius"]) == (lb.CONV_DIRECT, 13)
+    r = lb.inspect(preset("lenia_orbium.json"), 1280, 720, base_dir="/root/reference")
+    assert r["use_stamp_init"] == 1 and r["radius"] == 13
+
+
+def test_inspect_bad_json():
+    with pytest.raises(lb.LeniaError):
+        lb.inspect("{not json", 64, 64)

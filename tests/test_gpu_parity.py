@@ -1,0 +1,210 @@
+"""Parity of the CUDA path (called through the C ABI) with the reference.
+
+Anchors, in order of strength:
+* the reference's own outputs (tests/golden, produced by the reference's
+  Lenia.cpp and Metal kernels compiled for the CPU);
+* the FP32 restatement of the reference ("ref32", bit-exact with those);
+* the FP64 oracle (same update in double precision, exact convolution).
+Tolerances: integer hashing and the init passes are compared bit for bit;
+float fields within the bounds stated per test (the GPU sums taps in a
+different order and contracts multiply-adds, the FFT path rounds in a
+different pattern; the FP64 oracle is the accuracy reference).
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import life_simulation_b200 as lb
+from life_simulation_b200 import workloads as wl
+from oracle import lenia_oracle as lo
+from oracle.lenia_oracle import OracleLenia
+
+pytestmark = pytest.mark.gpu
+
+
+def organism_for(params):
+    if "organism" not in params:
+        return None
+    d = json.load(open(params["organism"]))
+    return lo.Organism(np.asarray(d["cells"], np.float32), d["R"], d["T"], d["mu"], d["sigma"])
+
+
+GOLDEN_TOL = {  # max |gpu - reference| per frame
+    "direct_basic": 2e-5, "direct_extras": 5e-5, "fft_multi": 2e-5, "fft_implicit": 2e-5,
+    "fft_fallback_nonpow2": 2e-5, "small_field_wrap": 2e-5,
+}
+
+
+@pytest.mark.parametrize("name", sorted(GOLDEN_TOL))
+def test_gpu_matches_reference_golden(golden, name):
+    d, man = golden
+    c = man[name]
+    m = lb.LeniaModule(c["params"], *c["scene"])
+    assert [m.width, m.height] == c["sim"]
+    m.reset(c["seed"])
+    want = d[name + "/fields"]
+    for i, (f, sub, af) in enumerate(c["frames"]):
+        m.encode(f, sub, af)
+        err = np.abs(m.field() - want[i]).max()
+        assert err <= GOLDEN_TOL[name], (name, f, err)
+
+
+@pytest.mark.parametrize("name", ["stamp_init", "noise_init"])
+def test_gpu_init_bit_exact(golden, name):
+    d, man = golden
+    c = man[name]
+    m = lb.LeniaModule(c["params"], *c["scene"])
+    m.reset(c["seed"])
+    f, sub, af = c["frames"][0]
+    m.encode(f, sub, af)  # dt = 0: the field after the frame is the init
+    np.testing.assert_array_equal(m.field(), d[name + "/fields"][0])
+
+
+def run_pair(params, w, h, init, steps, precision="f64", substeps=1, seed=3, frame0=0):
+    """Steps the GPU module and the oracle from the same field; yields both."""
+    m = lb.LeniaModule(params, w, h)
+    o = OracleLenia(params, w, h, precision)
+    m.reset(seed)
+    o.reset(seed)
+    if init is not None:
+        m.upload(init)
+        o.set_initial_field(init)
+    for s in range(steps):
+        m.encode(frame0 + s, substeps)
+        yield m.field(), o.encode(frame0 + s, substeps)
+
+
+def test_noise_and_injection_hash_patterns():
+    # Growth switched off (dt = 0): the step adds only the hashed noise and
+    # blends in the hashed blobs, so any hash difference shows at O(1e-2).
+    p = {"radius": 5, "dt": 0.0, "noiseAmount": 1.0, "injectAmount": 0.8, "injectCount": 6,
+         "growthMode": 0}
+    init = np.full((70, 90), 0.5, np.float32)
+    for g, o in run_pair(p, 90, 70, init, 3, "ref32"):
+        assert np.abs(g - o).max() < 1e-6
+
+
+def test_mu_jitter_uses_audio_frame():
+    p = {"radius": 6, "dt": 0.3, "muJitter": 1.0, "growthMode": 0, "growthSigma": 0.05}
+    rng = np.random.default_rng(1)
+    init = rng.random((64, 64)).astype(np.float32)
+    m = lb.LeniaModule(p, 64, 64)
+    o = OracleLenia(p, 64, 64, "f64")
+    for x in (m, o):
+        x.reset(9)
+    m.upload(init)
+    o.set_initial_field(init)
+    m.encode(4, 1, 77)
+    want = o.encode(4, 1, 77)
+    assert np.abs(m.field() - want).max() < 1e-5
+
+
+def test_direct_single_256_100_steps_vs_fp64():
+    params, w, h, init = wl.workload("single_256")
+    worst = 0.0
+    for s, (g, o) in enumerate(run_pair(params, w, h, init, 100)):
+        worst = max(worst, float(np.abs(g - o).max()))
+    assert worst <= 1e-5, worst
+
+
+@pytest.mark.parametrize("w,h,mode", [(128, 64, 1), (120, 90, 0), (96, 60, 0), (64, 48, 1)])
+def test_fft_vs_fp64_oracle(w, h, mode):
+    p = wl.fft3_params(w, h)
+    p["growthMode"] = mode
+    p["radius"] = 12
+    init = wl.patches(w, h, 6, 24, seed=5)
+    worst = 0.0
+    for g, o in run_pair(p, w, h, init, 20):
+        worst = max(worst, float(np.abs(g - o).max()))
+    assert worst <= 1e-5, worst
+
+
+def test_fft_extras_vs_ref32():
+    # injection, noise and jitter through the FFT path's growth epilogue
+    p = {"convMode": "fft", "radius": 9, "dt": 0.2, "growthMode": 1, "noiseAmount": 0.4,
+         "muJitter": 0.6, "injectAmount": 0.5, "injectCount": 3,
+         "kernels": [{"mu": 0.15, "sigma": 0.02, "weight": 0.7, "betas": [1.0]},
+                     {"radiusScale": 0.6, "mu": 0.25, "sigma": 0.04, "weight": 0.3, "betas": [1.0, 0.5]}]}
+    rng = np.random.default_rng(2)
+    init = (rng.random((64, 128)) * 0.6).astype(np.float32)
+    for g, o in run_pair(p, 128, 64, init, 5, "ref32"):
+        assert np.abs(g - o).max() < 2e-5
+
+
+@pytest.mark.parametrize("w,h", [(256, 256), (120, 90), (384, 216)])
+def test_direct_and_fft_agree_per_step(w, h):
+    pf = wl.fft3_params(w, h)
+    pd = wl.fft3_params(w, h, conv="directMulti")
+    init = wl.patches(w, h, 8, 40, seed=4)
+    mf, md = lb.LeniaModule(pf, w, h), lb.LeniaModule(pd, w, h)
+    for m in (mf, md):
+        m.reset(1)
+    a = init
+    worst = 0.0
+    for s in range(10):
+        mf.upload(a)
+        md.upload(a)
+        mf.encode(s)
+        md.encode(s)
+        f, d = mf.field(), md.field()
+        worst = max(worst, float(np.abs(f - d).max()))
+        a = f
+    assert worst <= 1e-5, worst
+
+
+def test_determinism_same_seed_same_bits():
+    p = wl.fft3_params(240, 120)
+    p["noiseAmount"] = 0.2
+    runs = []
+    for _ in range(2):
+        m = lb.LeniaModule(p, 240, 120)
+        m.reset(1234)
+        for f in range(5):
+            m.encode(f, 2)
+        runs.append(m.field())
+    np.testing.assert_array_equal(runs[0], runs[1])
+
+
+def test_upload_download_roundtrip_and_device_copy():
+    m = lb.LeniaModule({"radius": 4}, 37, 23)
+    a = np.random.default_rng(3).random((23, 37)).astype(np.float32)
+    m.upload(a)
+    np.testing.assert_array_equal(m.field(), a)
+    assert m.field_device_ptr() != 0
+    with pytest.raises(ValueError):
+        m.upload(np.zeros(10, np.float32))
+
+
+def test_params_table_and_overrides():
+    p = {"radius": 7, "dt": 0.25, "growthMu": 0.2, "growthMode": 0}
+    m = lb.LeniaModule(p, 48, 48)
+    fp = m.frame_params(3)
+    assert abs(fp.dt - 0.25) < 1e-7 and fp.growth_mode == 0 and fp.inject_count == 3
+    m.set_override("dt", 0.5)
+    assert abs(m.frame_params(3).dt - 0.5) < 1e-7
+    m.clear_override("dt")
+    m.set_param("growthSigma", 0.03)
+    fp = m.frame_params(3)
+    assert abs(fp.growth_sigma - 0.03) < 1e-7 and abs(fp.dt - 0.25) < 1e-7
+
+
+def test_fft_falls_back_to_direct_like_reference(golden):
+    d, man = golden
+    c = man["fft_fallback_nonpow2"]
+    m = lb.LeniaModule(c["params"], *c["scene"])
+    assert "powers of two" in m.warning and m.info()["conv_mode"] == lb.CONV_DIRECT
+
+
+def test_radius_beyond_direct_limit_is_an_error():
+    with pytest.raises(lb.LeniaError):
+        lb.LeniaModule({"radius": 40}, 128, 128)
+
+
+def test_zero_radius_and_tiny_fields():
+    for p, w, h in [({"radius": 0, "growthMode": 0}, 16, 16), ({"radius": 13}, 7, 5),
+                    ({"convMode": "fft", "radius": 3}, 8, 4)]:
+        init = np.random.default_rng(w).random((h, w)).astype(np.float32)
+        for g, o in run_pair(p, w, h, init, 3, "ref32"):
+            assert np.abs(g - o).max() < 2e-5, (p, w, h)
