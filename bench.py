@@ -118,7 +118,7 @@ class ClockSampler:
         sm = [float(r[1]) for r in self.rows if r[1].replace(".", "", 1).isdigit()]
         mx = [float(r[2]) for r in self.rows if r[2].replace(".", "", 1).isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in self.rows for i in range(4) if "Active" in r[5 + i]})
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[5 + i] == "Active"})
         return {"sm_mhz": statistics.median(sm) if sm else None,
                 "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(self.rows)}
 
@@ -242,7 +242,10 @@ def run_b200(args):
     m = lb.LeniaModule(params, w, h)
     m.reset(2 + rank)
     m.upload(init)
-    stream = torch.cuda.current_stream()
+    # A dedicated stream: handle 0 (the legacy default stream) would mean
+    # "the context's own stream" to the C ABI.
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     sh = stream.cuda_stream
     fp = m.frame_params(0)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")

@@ -37,6 +37,18 @@ __device__ __forceinline__ float bell(float u, float mu, float sigma) {
     return expf(-0.5f * t * t);
 }
 
+// The same bell with a precomputed 1/sigma and one hardware base-2
+// exponential: exp(-0.5 t^2) = 2^(-0.5 log2(e) t^2). ex2.approx.ftz has a
+// relative error below 2^-22 (negligible against the FP32 FFT's rounding),
+// and it replaces an IEEE division and the full-range expf sequence; used on
+// the spectral path, where the growth map is a large share of the row pass.
+__device__ __forceinline__ float bell_fast(float u, float mu, float inv_sigma) {
+    const float t = (u - mu) * inv_sigma;
+    float r;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(-0.72134752044448170368f * t * t));
+    return r;
+}
+
 // Running growth sums over kernels in the reference's order
 // (Lenia.metal:188-195): sum_k h_k*bell_k and sum_k h_k*(2*bell_k - 1).
 struct GrowthAcc {

@@ -5,6 +5,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <vector>
 
 #include "lenia_types.h"
 
@@ -63,6 +64,28 @@ cudaError_t launch_row_c2r_growth(const FftGeometry& g, const float2* U, const f
                                   cudaStream_t s);
 size_t fft_row_smem_bytes(const FftGeometry& g);
 size_t fft_col_smem_bytes(const FftGeometry& g);
+
+// Compile-time-plan passes (lenia_fft_fast.cu) for the sizes they cover.
+struct FastPlan {
+    int n = 0;
+    int np = 0;
+    int radix[kMaxPasses] = {};
+};
+struct FastTables {
+    const float2* col_twf = nullptr;  // column forward plan, per-pass twiddles
+    const float2* col_twi = nullptr;  // column inverse plan (reversed passes)
+    const float2* row_twi = nullptr;  // row inverse plan
+    const float2* row_twf = nullptr;  // row forward plan (reversed passes)
+};
+bool fast_col_plan(int H, FastPlan& forward_plan);
+bool fast_row_plan(int M, FastPlan& inverse_plan);
+void fast_plan_twiddles(const FastPlan& plan, std::vector<float2>& out);
+// batch: columns (rows) per CTA iteration, 1, 2 or 4.
+cudaError_t launch_col_fast(const FftGeometry& g, const FastTables& t, int batch, const float2* S,
+                            float2* U, cudaStream_t s);
+cudaError_t launch_row_fast(const FftGeometry& g, const FastTables& t, int batch, const float2* U,
+                            const float* A, float* A_out, float2* S_next, const StepParams& p,
+                            cudaStream_t s);
 
 // ------------------------------------------------------------------ inits
 cudaError_t launch_init_noise(float* A, const InitParams& p, cudaStream_t s);

@@ -427,6 +427,9 @@ void LeniaModule::release() {
     rel(d_tw_row_);
     rel(d_tw_col_);
     rel(d_tw_r2c_);
+    for (auto& t : d_fast_tw_) rel(t);
+    fast_col_ = fast_row_ = false;
+    fast_ = FastTables();
     d_weights_ = nullptr;
     d_spans_ = nullptr;
     d_org_ = nullptr;
@@ -727,6 +730,85 @@ int LeniaModule::buildSpectralTables(const std::vector<KernelDef>& eff) {
     fgeo_.tw_r2c = d_tw_r2c_;
     fgeo_.khat = d_khat_;
     num_k_ = nk;
+
+    // Compile-time-plan passes where this size has one; per-pass twiddle
+    // tables for the plan and its reverse.
+    FastPlan cf, ri;
+    fast_col_ = fast_col_plan(H, cf);
+    fast_row_ = fast_row_plan(M, ri);
+    auto upload_plan = [&](const FastPlan& pl, float2*& dst) -> int {
+        std::vector<float2> tw;
+        fast_plan_twiddles(pl, tw);
+        if (tw.empty()) tw.push_back(make_float2(1.0f, 0.0f));
+        if ((e = dev_alloc(&dst, tw.size(), device_bytes_)) != cudaSuccess) return cudaFail(e, "cudaMalloc twiddles");
+        cudaMemcpy(dst, tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice);
+        return LENIA_OK;
+    };
+    auto reversed = [](const FastPlan& pl) {
+        FastPlan r = pl;
+        for (int i = 0; i < pl.np; ++i) r.radix[i] = pl.radix[pl.np - 1 - i];
+        return r;
+    };
+    if (fast_col_) {
+        if (upload_plan(cf, d_fast_tw_[0]) < 0 || upload_plan(reversed(cf), d_fast_tw_[1]) < 0) return LENIA_ERR_CUDA;
+        fast_.col_twf = d_fast_tw_[0];
+        fast_.col_twi = d_fast_tw_[1];
+    }
+    if (fast_row_) {
+        if (upload_plan(ri, d_fast_tw_[2]) < 0 || upload_plan(reversed(ri), d_fast_tw_[3]) < 0) return LENIA_ERR_CUDA;
+        fast_.row_twi = d_fast_tw_[2];
+        fast_.row_twf = d_fast_tw_[3];
+    }
+    return autotuneSpectral();
+}
+
+// Picks columns (rows) per CTA of the compile-time-plan passes by timing
+// each candidate on this context's own buffers (contents irrelevant).
+int LeniaModule::autotuneSpectral() {
+    if (!fast_col_ && !fast_row_) return LENIA_OK;
+    cudaEvent_t a = takeEvent(), b = takeEvent();
+    StepParams p{};
+    p.num_kernels = uint32_t(fgeo_.nk);
+    p.width = w_;
+    p.height = h_;
+    p.sigma[0] = p.sigma[1] = p.sigma[2] = p.sigma[3] = 1.0f;
+    auto time_it = [&](auto&& fn) {
+        float best = 1e30f;
+        for (int rep = 0; rep < 4; ++rep) {
+            cudaEventRecord(a, stream_);
+            if (fn() != cudaSuccess) return 1e30f;
+            cudaEventRecord(b, stream_);
+            cudaEventSynchronize(b);
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, a, b);
+            if (rep > 0) best = std::min(best, ms);
+        }
+        return best;
+    };
+    const int cands[3] = {1, 2, 4};
+    if (fast_col_) {
+        float best = 1e30f;
+        for (int c : cands) {
+            const float t = time_it([&] { return launch_col_fast(fgeo_, fast_, c, d_S_, d_U_, stream_); });
+            if (t < best) { best = t; col_batch_ = c; }
+        }
+        if (best >= 1e29f) fast_col_ = false;
+    }
+    if (fast_row_) {
+        float best = 1e30f;
+        for (int c : cands) {
+            const float t = time_it([&] {
+                return launch_row_fast(fgeo_, fast_, c, d_U_, field_[0], field_[1], d_S_, p, stream_);
+            });
+            if (t < best) { best = t; row_batch_ = c; }
+        }
+        if (best >= 1e29f) fast_row_ = false;
+    }
+    cudaGetLastError();
+    event_pool_.push_back(a);
+    event_pool_.push_back(b);
+    cudaMemsetAsync(field_[0], 0, sizeof(float) * w_ * h_, stream_);
+    cudaMemsetAsync(field_[1], 0, sizeof(float) * w_ * h_, stream_);
     return LENIA_OK;
 }
 
@@ -911,10 +993,15 @@ int LeniaModule::step(const lenia_frame_params& fp, uint32_t substeps, cudaStrea
                 e = launch(LENIA_PHASE_ROW_FFT, s, [&] { return launch_row_r2c(fgeo_, src, d_S_, s); });
                 if (e != cudaSuccess) return cudaFail(e, "row pass");
             }
-            e = launch(LENIA_PHASE_COLUMN, s, [&] { return launch_col_conv(fgeo_, d_S_, d_U_, s); });
+            e = launch(LENIA_PHASE_COLUMN, s, [&] {
+                return fast_col_ ? launch_col_fast(fgeo_, fast_, col_batch_, d_S_, d_U_, s)
+                                 : launch_col_conv(fgeo_, d_S_, d_U_, s);
+            });
             if (e != cudaSuccess) return cudaFail(e, "column pass");
-            e = launch(LENIA_PHASE_ROW_GROWTH, s,
-                       [&] { return launch_row_c2r_growth(fgeo_, d_U_, src, dst, d_S_, p, s); });
+            e = launch(LENIA_PHASE_ROW_GROWTH, s, [&] {
+                return fast_row_ ? launch_row_fast(fgeo_, fast_, row_batch_, d_U_, src, dst, d_S_, p, s)
+                                 : launch_row_c2r_growth(fgeo_, d_U_, src, dst, d_S_, p, s);
+            });
             if (e != cudaSuccess) return cudaFail(e, "growth pass");
             spectrum_valid_ = true;
         } else {

@@ -142,6 +142,7 @@ private:
     int cudaFail(cudaError_t e, const char* where);
     int buildDirectTables();
     int buildSpectralTables(const std::vector<KernelDef>& eff);
+    int autotuneSpectral();
     int initField(const lenia_frame_params& fp, cudaStream_t s);
     int initKernels(const lenia_frame_params& fp);
     void fillStepParams(const lenia_frame_params& fp, uint32_t seed, StepParams& p) const;
@@ -192,6 +193,10 @@ private:
     int direct_tile_ = kDirectTile64x16;
     int direct_nk_ = 1;
     FftGeometry fgeo_{};
+    bool fast_col_ = false, fast_row_ = false;  // compile-time-plan passes
+    int col_batch_ = 2, row_batch_ = 2;         // autotuned per size
+    FastTables fast_{};
+    float2* d_fast_tw_[4] = {nullptr, nullptr, nullptr, nullptr};
 
     // Launch accounting and profiling.
     uint64_t launches_ = 0;
