@@ -21,13 +21,19 @@
 namespace lenia {
 namespace fft {
 
-__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+// Complex arithmetic on float2 with the packed FP32x2 instructions of sm_100
+// (one add/mul/fma per complex lane pair instead of two); each lane is an
+// IEEE round-to-nearest operation, the same result as the scalar form.
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) {
+    return __ffma2_rn(b, make_float2(-1.0f, -1.0f), a);
+}
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
-    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+    const float2 t = __fmul2_rn(make_float2(a.x, a.x), b);
+    return __ffma2_rn(make_float2(-a.y, a.y), make_float2(b.y, b.x), t);
 }
 __device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
-__device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+__device__ __forceinline__ float2 cscale(float2 a, float s) { return __fmul2_rn(a, make_float2(s, s)); }
 // -i*a (forward quarter turn) and +i*a.
 __device__ __forceinline__ float2 mul_mi(float2 a) { return make_float2(a.y, -a.x); }
 __device__ __forceinline__ float2 mul_pi(float2 a) { return make_float2(-a.y, a.x); }
@@ -58,7 +64,7 @@ template <bool INV>
 __device__ __forceinline__ void dft3(float2* v) {
     float2 t = cadd(v[1], v[2]);
     float2 d = csub(v[1], v[2]);
-    float2 m = make_float2(v[0].x + kC3 * t.x, v[0].y + kC3 * t.y);
+    float2 m = __ffma2_rn(t, make_float2(kC3, kC3), v[0]);
     v[0] = cadd(v[0], t);
     float2 r = rot90<INV>(cscale(d, kS3));  // -i*s*d forward
     v[1] = cadd(m, r);
@@ -81,10 +87,12 @@ __device__ __forceinline__ void dft5(float2* v) {
     float2 a2 = cadd(v[2], v[3]), b2 = csub(v[2], v[3]);
     float2 x0 = v[0];
     v[0] = cadd(x0, cadd(a1, a2));
-    float2 c1 = make_float2(x0.x + kC51 * a1.x + kC52 * a2.x, x0.y + kC51 * a1.y + kC52 * a2.y);
-    float2 c2 = make_float2(x0.x + kC52 * a1.x + kC51 * a2.x, x0.y + kC52 * a1.y + kC51 * a2.y);
-    float2 s1 = rot90<INV>(make_float2(kS51 * b1.x + kS52 * b2.x, kS51 * b1.y + kS52 * b2.y));
-    float2 s2 = rot90<INV>(make_float2(kS52 * b1.x - kS51 * b2.x, kS52 * b1.y - kS51 * b2.y));
+    const float2 C51 = make_float2(kC51, kC51), C52 = make_float2(kC52, kC52);
+    const float2 S51 = make_float2(kS51, kS51), S52 = make_float2(kS52, kS52);
+    float2 c1 = __ffma2_rn(a2, C52, __ffma2_rn(a1, C51, x0));
+    float2 c2 = __ffma2_rn(a2, C51, __ffma2_rn(a1, C52, x0));
+    float2 s1 = rot90<INV>(__ffma2_rn(b2, S52, __fmul2_rn(b1, S51)));
+    float2 s2 = rot90<INV>(__ffma2_rn(b2, make_float2(-kS51, -kS51), __fmul2_rn(b1, S52)));
     v[1] = cadd(c1, s1);
     v[4] = csub(c1, s1);
     v[2] = cadd(c2, s2);
@@ -94,13 +102,17 @@ __device__ __forceinline__ void dft5(float2* v) {
 // w_8^k for k = 1, 2, 3 applied to b (forward w = exp(-i*pi/4)).
 template <bool INV>
 __device__ __forceinline__ float2 w8_1(float2 b) {
-    return INV ? make_float2(kS2 * (b.x - b.y), kS2 * (b.x + b.y))
-               : make_float2(kS2 * (b.x + b.y), kS2 * (b.y - b.x));
+    // (b.x -/+ b.y, b.x +/- b.y) * sqrt(1/2)
+    const float2 s = INV ? __ffma2_rn(make_float2(b.y, b.y), make_float2(-1.0f, 1.0f), make_float2(b.x, b.x))
+                         : __ffma2_rn(make_float2(b.x, b.x), make_float2(1.0f, -1.0f), make_float2(b.y, b.y));
+    return __fmul2_rn(s, make_float2(kS2, kS2));
 }
 template <bool INV>
 __device__ __forceinline__ float2 w8_3(float2 b) {
-    return INV ? make_float2(-kS2 * (b.x + b.y), kS2 * (b.x - b.y))
-               : make_float2(kS2 * (b.y - b.x), -kS2 * (b.x + b.y));
+    // forward: sqrt(1/2) * (b.y - b.x, -(b.x + b.y)); inverse: sqrt(1/2) * (-(b.x + b.y), b.x - b.y)
+    const float2 s = INV ? __ffma2_rn(make_float2(b.y, b.y), make_float2(-1.0f, -1.0f), make_float2(-b.x, b.x))
+                         : __ffma2_rn(make_float2(b.x, b.x), make_float2(-1.0f, -1.0f), make_float2(b.y, -b.y));
+    return __fmul2_rn(s, make_float2(kS2, kS2));
 }
 
 template <bool INV>

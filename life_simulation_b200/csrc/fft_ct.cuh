@@ -83,7 +83,8 @@ __device__ __forceinline__ float2 twmul(float2 a) {
         return INV ? fft::mul_mi(a) : fft::mul_pi(a);
     } else {
         constexpr float wr = Tw<p, Q, INV>::re, wi = Tw<p, Q, INV>::im;
-        return make_float2(a.x * wr - a.y * wi, a.x * wi + a.y * wr);
+        const float2 t = __fmul2_rn(make_float2(a.x, a.x), make_float2(wr, wi));
+        return __ffma2_rn(make_float2(a.y, a.y), make_float2(-wi, wr), t);
     }
 }
 

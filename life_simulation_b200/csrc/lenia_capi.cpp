@@ -18,6 +18,10 @@ struct lenia_ctx {
 
 namespace {
 
+// Message of the last failed create/inspect on this thread
+// (lenia_last_message(NULL)).
+thread_local std::string g_create_error;
+
 int set_msg(lenia_ctx* c, int rc) {
     if (c) c->message = c->module.message();
     return rc;
@@ -40,6 +44,7 @@ int finish_create(lenia_ctx* c, uint32_t w, uint32_t h, lenia_ctx** out) {
     const int rc = c->module.setup(w, h);
     c->message = c->module.message();
     if (rc < 0) {
+        g_create_error = c->message;
         delete c;
         *out = nullptr;
         return rc;
@@ -47,8 +52,6 @@ int finish_create(lenia_ctx* c, uint32_t w, uint32_t h, lenia_ctx** out) {
     *out = c;
     return rc;
 }
-
-thread_local std::string g_create_error;
 
 }  // namespace
 

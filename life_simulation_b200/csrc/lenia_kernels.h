@@ -66,6 +66,11 @@ size_t fft_row_smem_bytes(const FftGeometry& g);
 size_t fft_col_smem_bytes(const FftGeometry& g);
 
 // Compile-time-plan passes (lenia_fft_fast.cu) for the sizes they cover.
+// They use the blocked spectral layout: element (kx, ky) of a plane at
+// ((kx / kSpectralBlock) * H + ky) * kSpectralBlock + kx % kSpectralBlock
+// (M must be a multiple of kSpectralBlock); the runtime-plan kernels above
+// use the column-major layout. A context uses one or the other throughout.
+constexpr int kSpectralBlock = 8;
 struct FastPlan {
     int n = 0;
     int np = 0;
@@ -80,12 +85,14 @@ struct FastTables {
 bool fast_col_plan(int H, FastPlan& forward_plan);
 bool fast_row_plan(int M, FastPlan& inverse_plan);
 void fast_plan_twiddles(const FastPlan& plan, std::vector<float2>& out);
-// batch: columns (rows) per CTA iteration, 1, 2 or 4.
+// batch: columns per CTA iteration (2, 4 or 8) / rows per CTA iteration
+// (1, 2 or 4). launch_row_fast with nk = 0 computes only the row spectrum of
+// A into S_next (U, A_out unused).
 cudaError_t launch_col_fast(const FftGeometry& g, const FastTables& t, int batch, const float2* S,
                             float2* U, cudaStream_t s);
 cudaError_t launch_row_fast(const FftGeometry& g, const FastTables& t, int batch, const float2* U,
                             const float* A, float* A_out, float2* S_next, const StepParams& p,
-                            cudaStream_t s);
+                            int nk, cudaStream_t s);
 
 // ------------------------------------------------------------------ inits
 cudaError_t launch_init_noise(float* A, const InitParams& p, cudaStream_t s);
