@@ -219,6 +219,41 @@ typedef struct lenia_profile_data {
 } lenia_profile_data;
 int lenia_profile(lenia_ctx* ctx, int enable);
 int lenia_profile_read(lenia_ctx* ctx, lenia_profile_data* out);
+/* ---- One spectral substep without device allocation ----
+ * No counterpart in the reference (its module always owns its textures).
+ *
+ * For callers that cannot allocate device memory at the point where they
+ * step the field: a real-time frame callback, where cudaMalloc/cudaFree can
+ * synchronise the whole device and stall the frame, or a host application
+ * that reserves the GPU's memory up front and hands out only its own
+ * buffers. The caller owns the field buffers; everything else the step needs
+ * (row spectrum, per-kernel potentials, kernel spectra, FFT twiddle tables)
+ * lives in one static device array of LENIA_NOALLOC_SCRATCH_BYTES (8 MiB),
+ * which every GPU that loads this library holds until the process exits.
+ * No call allocates or frees device memory.
+ *
+ * field_in, field_out: distinct device buffers of height x width floats.
+ * cfg: kernels, num_kernels (0: one kernel from fp's growth mu/sigma),
+ *   radius, kernel_shell_sigma, kernel_core; its other fields are unused.
+ * fp: the per-frame values; seed: the substep seed (the module uses
+ *   pcgHash(deriveSeed(reset_seed) ^ (frame_index*197 + substep))).
+ * Sizes: even width, width/2 and height with prime factors 2, 3, 5 only, and
+ *   4*W*H*(1 + K) + 4*K*(W/2+1)*(H/2+1) bytes plus small tables must fit in
+ *   the array (e.g. 512x512 with 4 kernels); larger fields return
+ *   LENIA_ERR_UNSUPPORTED and lenia_noalloc_last_message() says why.
+ * The first call on a device, and the first call after the field size or the
+ * kernel shapes change, builds the kernel spectra on the host and copies
+ * them into the array synchronously on `stream`; other calls only queue
+ * kernels on `stream`. All calls share the one array and each call fully
+ * rewrites the parts it reads, so nothing needs clearing, but calls that
+ * overlap on the GPU (other streams or host threads) race on it. */
+#define LENIA_NOALLOC_SCRATCH_BYTES (8u * 1024u * 1024u)
+int lenia_fft_step_noalloc(const float* field_in, float* field_out, uint32_t width, uint32_t height,
+                           const lenia_config* cfg, const lenia_frame_params* fp, uint32_t seed,
+                           void* stream);
+/* Message of the calling thread's last failed lenia_fft_step_noalloc. */
+const char* lenia_noalloc_last_message(void);
+
 /* Message of the last warning or error on this context ("" if none). */
 const char* lenia_last_message(lenia_ctx* ctx);
 const char* lenia_status_string(int status);

@@ -91,6 +91,7 @@ EXPORTS = (
     "lenia_download_device", "lenia_field_device_ptr", "lenia_get_info",
     "lenia_get_stream", "lenia_profile", "lenia_profile_read",
     "lenia_last_message", "lenia_status_string",
+    "lenia_fft_step_noalloc", "lenia_noalloc_last_message",
 )
 
 PHASES = ("init", "direct", "row_fft", "column", "row_growth")
@@ -141,6 +142,10 @@ def load_library(path: str = LIB_PATH):
     L.lenia_last_message.restype = ctypes.c_char_p
     L.lenia_status_string.argtypes = [i32]
     L.lenia_status_string.restype = ctypes.c_char_p
+    L.lenia_fft_step_noalloc.argtypes = [P, P, u32, u32, ctypes.POINTER(Config),
+                                         ctypes.POINTER(FrameParams), u32, P]
+    L.lenia_noalloc_last_message.argtypes = []
+    L.lenia_noalloc_last_message.restype = ctypes.c_char_p
     for name in EXPORTS:
         getattr(L, name)  # raises AttributeError if the build lacks a symbol
     _LIB = L
