@@ -57,6 +57,9 @@ def parse_args():
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--mode", choices=["step", "sweep"], default="step",
+                    help="step: the 1080p headline; sweep: the 512-world batched sweep")
+    ap.add_argument("--plain-steps", type=int, default=10)
     return ap.parse_args()
 
 
@@ -348,10 +351,79 @@ def run_b200(args):
     return 0
 
 
+def run_sweep(args):
+    """512 worlds of mixed sizes, 240 substeps with the
+    activity readback every 60, batched (one graph per 60 substeps) against
+    the plain form (one context per world, worlds stepped one at a time)."""
+    import torch
+
+    import life_simulation_b200 as lb
+    from life_simulation_b200 import workloads as wl
+
+    torch.cuda.set_device(0)
+    specs, inits = wl.sweep512()
+    worlds = [lb.make_world(s["width"], s["height"], s["radius"], s["mu"], s["sigma"], s["dt"], 0,
+                            seed=s["seed"]) for s in specs]
+    px = sum(w.width * w.height for w in worlds)
+    b = lb.LeniaBatch(worlds, lb.BATCH_AUTO)
+    for i, a in enumerate(inits):
+        b.upload(i, a)
+    b.step(60)  # warm-up (also captures the graph)
+    b.sync()
+    for i, a in enumerate(inits):
+        b.upload(i, a)
+    b.step(0)
+    b.sync()
+    t0 = time.perf_counter()
+    for _ in range(4):
+        b.step(60)
+        b.stats()  # synchronising activity readback
+    batched_s = time.perf_counter() - t0
+    paths = [b.path(i) for i in range(len(worlds))]
+    b.close()
+    # Plain form: one context per world (its own kernel launches), the same
+    # path per world, worlds stepped one after another for a sample of steps.
+    plain_steps = args.plain_steps
+    mods = []
+    for i, w in enumerate(worlds):
+        conv = "fft" if paths[i] == lb.CONV_FFT else "direct"
+        m = lb.LeniaModule(lb.single_world_params(w, conv), w.width, w.height)
+        m.reset(w.seed)
+        m.upload(inits[i])
+        mods.append(m)
+    # All contexts on one stream, so worlds run one after another as in the
+    # reference's variant loop (no overlap between worlds on the device).
+    one = torch.cuda.Stream()
+    sh = one.cuda_stream
+    for m in mods:
+        m.encode(0, 1, stream=sh)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for m in mods:
+        for f in range(plain_steps):
+            m.encode(1 + f, 1, stream=sh)
+    torch.cuda.synchronize()
+    plain_s = time.perf_counter() - t0
+    for m in mods:
+        m.close()
+    batched = px * 240 / batched_s / 1e6
+    plain = px * plain_steps / plain_s / 1e6
+    print(json.dumps({
+        "metric": "Lenia Mpixel-steps/s, 512-world sweep (batched vs one world at a time)",
+        "unit": UNIT, "value": batched, "plain": plain, "speedup": batched / plain,
+        "worlds": len(worlds), "pixels_per_step": px, "steps": 240,
+        "direct_worlds": paths.count(lb.CONV_DIRECT), "fft_worlds": paths.count(lb.CONV_FFT),
+        "timing": "wall clock incl. 4 activity readbacks (batched); plain: "
+                  f"{plain_steps} substeps per world, worlds in sequence"}))
+    return 0
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.mode == "sweep":
+        return run_sweep(args)
     return run_b200(args)
 
 

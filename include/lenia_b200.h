@@ -219,6 +219,43 @@ typedef struct lenia_profile_data {
 } lenia_profile_data;
 int lenia_profile(lenia_ctx* ctx, int enable);
 int lenia_profile_read(lenia_ctx* ctx, lenia_profile_data* out);
+/* ---- Many worlds at once (batched sweep) ----
+ * Replaces the reference's one-world-at-a-time variant loop
+ * (Apps/LifePresetLab/main.cpp:718-795, a SceneRunner per variant): n
+ * independent worlds of any sizes and parameters, each a single-ring Lenia
+ * (the direct module's kernel, Lenia.cpp:410-446), stepped together. A
+ * substep of the whole batch is one direct launch over every direct world
+ * plus one column and one row launch per field size with spectral worlds;
+ * lenia_batch_step replays k substeps as one captured CUDA graph. The path of
+ * each world is chosen at creation: LENIA_BATCH_AUTO times the direct and
+ * spectral passes on the batch's own buffers and gives each world the
+ * cheaper one. Each world evolves exactly as it would alone. */
+typedef struct lenia_world {
+    uint32_t width, height;
+    uint32_t radius;          /* kernel radius (px) */
+    float mu, sigma, dt;      /* growth centre, width, time step */
+    uint32_t growth_mode;     /* 0 standard, 1 asymptotic */
+    uint32_t kernel_core;     /* LENIA_CORE_* */
+    float shell_mu, shell_sigma; /* Gaussian shell (reference defaults 0.5, 0.15) */
+    uint32_t seed;            /* reset seed: deriveSeed(seed, "LEN1") for the substep seeds */
+} lenia_world;
+enum { LENIA_BATCH_AUTO = 0, LENIA_BATCH_DIRECT = 1, LENIA_BATCH_FFT = 2 };
+typedef struct lenia_batch lenia_batch;
+int lenia_batch_create(const lenia_world* worlds, uint32_t n, uint32_t policy, lenia_batch** out);
+int lenia_batch_destroy(lenia_batch* b);
+/* Field of one world, height x width floats (host memory). */
+int lenia_batch_upload(lenia_batch* b, uint32_t world, const float* host);
+int lenia_batch_download(lenia_batch* b, uint32_t world, float* host);
+/* `steps` substeps of every world (frame indices advance by one per substep,
+ * seeds as the single-world module's). Asynchronous on `stream`. */
+int lenia_batch_step(lenia_batch* b, uint32_t steps, void* stream);
+/* Activity of every world: mean and variance of its field (n doubles each). */
+int lenia_batch_stats(lenia_batch* b, double* mean, double* var);
+/* LENIA_CONV_DIRECT or LENIA_CONV_FFT: the path the batch gave a world. */
+int lenia_batch_world_path(lenia_batch* b, uint32_t world, uint32_t* path);
+int lenia_batch_sync(lenia_batch* b);
+const char* lenia_batch_last_message(lenia_batch* b);
+
 /* ---- One spectral substep without device allocation ----
  * No counterpart in the reference (its module always owns its textures).
  *

@@ -92,7 +92,20 @@ EXPORTS = (
     "lenia_get_stream", "lenia_profile", "lenia_profile_read",
     "lenia_last_message", "lenia_status_string",
     "lenia_fft_step_noalloc", "lenia_noalloc_last_message",
+    "lenia_batch_create", "lenia_batch_destroy", "lenia_batch_upload", "lenia_batch_download",
+    "lenia_batch_step", "lenia_batch_stats", "lenia_batch_world_path", "lenia_batch_sync",
+    "lenia_batch_last_message",
 )
+
+BATCH_AUTO, BATCH_DIRECT, BATCH_FFT = 0, 1, 2
+
+
+class World(ctypes.Structure):
+    """lenia_world: one world of a batch (single-ring Lenia)."""
+    _fields_ = [("width", ctypes.c_uint32), ("height", ctypes.c_uint32), ("radius", ctypes.c_uint32),
+                ("mu", ctypes.c_float), ("sigma", ctypes.c_float), ("dt", ctypes.c_float),
+                ("growth_mode", ctypes.c_uint32), ("kernel_core", ctypes.c_uint32),
+                ("shell_mu", ctypes.c_float), ("shell_sigma", ctypes.c_float), ("seed", ctypes.c_uint32)]
 
 PHASES = ("init", "direct", "row_fft", "column", "row_growth")
 
@@ -146,6 +159,16 @@ def load_library(path: str = LIB_PATH):
                                          ctypes.POINTER(FrameParams), u32, P]
     L.lenia_noalloc_last_message.argtypes = []
     L.lenia_noalloc_last_message.restype = ctypes.c_char_p
+    L.lenia_batch_create.argtypes = [ctypes.POINTER(World), u32, u32, pp]
+    L.lenia_batch_destroy.argtypes = [P]
+    L.lenia_batch_upload.argtypes = [P, u32, P]
+    L.lenia_batch_download.argtypes = [P, u32, P]
+    L.lenia_batch_step.argtypes = [P, u32, P]
+    L.lenia_batch_stats.argtypes = [P, P, P]
+    L.lenia_batch_world_path.argtypes = [P, u32, ctypes.POINTER(u32)]
+    L.lenia_batch_sync.argtypes = [P]
+    L.lenia_batch_last_message.argtypes = [P]
+    L.lenia_batch_last_message.restype = ctypes.c_char_p
     for name in EXPORTS:
         getattr(L, name)  # raises AttributeError if the build lacks a symbol
     _LIB = L
@@ -366,3 +389,86 @@ def make_frame_params(dt=0.1, growth_mu=0.15, growth_sigma=0.017, noise_amount=0
     fp.frame_index = frame_index
     fp.audio_frame = frame_index if audio_frame is None else audio_frame
     return fp
+
+
+def make_world(width, height, radius, mu, sigma, dt, growth_mode=0, kernel_core=CORE_GAUSS_SHELL,
+               shell_mu=0.5, shell_sigma=0.15, seed=0) -> World:
+    w = World()
+    w.width, w.height, w.radius = width, height, radius
+    w.mu, w.sigma, w.dt, w.growth_mode, w.kernel_core = mu, sigma, dt, growth_mode, kernel_core
+    w.shell_mu, w.shell_sigma, w.seed = shell_mu, shell_sigma, seed
+    return w
+
+
+class LeniaBatch:
+    """Many independent worlds stepped together (lenia_batch_*)."""
+
+    def __init__(self, worlds, policy: int = BATCH_AUTO):
+        L = load_library()
+        self._L = L
+        self.worlds = list(worlds)
+        arr = (World * len(self.worlds))(*self.worlds)
+        self._h = ctypes.c_void_p()
+        rc = L.lenia_batch_create(arr, len(self.worlds), policy, ctypes.byref(self._h))
+        if rc < 0:
+            raise LeniaError(rc, "batch creation failed")
+
+    def _check(self, rc: int) -> int:
+        if rc < 0:
+            raise LeniaError(rc, self._L.lenia_batch_last_message(self._h).decode(errors="replace"))
+        return rc
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            self._L.lenia_batch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def upload(self, i: int, a: np.ndarray) -> None:
+        w = self.worlds[i]
+        a = np.ascontiguousarray(a, np.float32)
+        if a.size != w.width * w.height:
+            raise ValueError("field size mismatch")
+        self._check(self._L.lenia_batch_upload(self._h, i, a.ctypes.data_as(ctypes.c_void_p)))
+
+    def field(self, i: int) -> np.ndarray:
+        w = self.worlds[i]
+        out = np.empty((w.height, w.width), np.float32)
+        self._check(self._L.lenia_batch_download(self._h, i, out.ctypes.data_as(ctypes.c_void_p)))
+        return out
+
+    def step(self, steps: int = 1, stream: Optional[int] = None) -> None:
+        self._check(self._L.lenia_batch_step(self._h, steps, ctypes.c_void_p(stream) if stream else None))
+
+    def sync(self) -> None:
+        self._check(self._L.lenia_batch_sync(self._h))
+
+    def stats(self):
+        n = len(self.worlds)
+        mean = np.empty(n, np.float64)
+        var = np.empty(n, np.float64)
+        self._check(self._L.lenia_batch_stats(self._h, mean.ctypes.data_as(ctypes.c_void_p),
+                                              var.ctypes.data_as(ctypes.c_void_p)))
+        return mean, var
+
+    def path(self, i: int) -> int:
+        p = ctypes.c_uint32()
+        self._check(self._L.lenia_batch_world_path(self._h, i, ctypes.byref(p)))
+        return p.value
+
+
+def single_world_params(w: World, conv: str) -> dict:
+    """Scene params of a single-world context equivalent to batch world `w`."""
+    core = "exp" if w.kernel_core == CORE_EXP else "gaussShell"
+    p = {"radius": int(w.radius), "dt": w.dt, "growthMu": w.mu, "growthSigma": w.sigma,
+         "growthMode": int(w.growth_mode), "kernelCore": core, "kernelShellMu": w.shell_mu,
+         "kernelShellSigma": w.shell_sigma, "noiseAmount": 0.0, "muJitter": 0.0, "injectAmount": 0.0}
+    if conv == "fft":
+        p.update(convMode="fft", fftAnySize=True,
+                 kernels=[{"radiusScale": 1.0, "mu": w.mu, "sigma": w.sigma, "weight": 1.0, "betas": [1.0]}])
+    return p

@@ -43,12 +43,12 @@ __device__ __forceinline__ void unpack_span(uint32_t v, int& start, int& count) 
     count = int(v >> 16);
 }
 
+// One output tile at (x0, y0) of one world.
 template <int TW, int TH, int NK>
-__global__ void __launch_bounds__(DirectTile<TW, TH>::kThreads)
-    direct_step_kernel(const float* __restrict__ src, float* __restrict__ dst,
-                       const float* __restrict__ weights,  // [NK][2R+1][WP], zero padded
-                       const uint32_t* __restrict__ spans, // [NK][2R+1]
-                       DirectGeometry g, StepParams p) {
+__device__ __forceinline__ void direct_tile(const float* __restrict__ src, float* __restrict__ dst,
+                                            const float* __restrict__ weights,  // [NK][2R+1][WP], zero padded
+                                            const uint32_t* __restrict__ spans, // [NK][2R+1]
+                                            const DirectGeometry& g, const StepParams& p, int x0, int y0) {
     extern __shared__ __align__(16) float smem[];
     const int TP = TW + 2 * g.xp + 8;          // tile pitch (floats), multiple of 4
     const int TR = TH + 2 * g.r;               // tile rows
@@ -57,7 +57,6 @@ __global__ void __launch_bounds__(DirectTile<TW, TH>::kThreads)
     uint32_t* sp = reinterpret_cast<uint32_t*>(wts + NK * g.ksize * g.wp);
 
     const int W = int(p.width), H = int(p.height);
-    const int x0 = blockIdx.x * TW, y0 = blockIdx.y * TH;
     const int tid = threadIdx.x;
     constexpr int NT = DirectTile<TW, TH>::kThreads;
 
@@ -127,6 +126,27 @@ __global__ void __launch_bounds__(DirectTile<TW, TH>::kThreads)
 }
 
 template <int TW, int TH, int NK>
+__global__ void __launch_bounds__(DirectTile<TW, TH>::kThreads)
+    direct_step_kernel(const float* __restrict__ src, float* __restrict__ dst,
+                       const float* __restrict__ weights, const uint32_t* __restrict__ spans,
+                       DirectGeometry g, StepParams p) {
+    direct_tile<TW, TH, NK>(src, dst, weights, spans, g, p, blockIdx.x * TW, blockIdx.y * TH);
+}
+
+// Many worlds in one launch: CTA i computes tile tiles[i] = (world, tile x,
+// tile y) of that world; each world brings its own state buffers, LUT,
+// geometry and growth parameters.
+template <int TW, int TH>
+__global__ void __launch_bounds__(DirectTile<TW, TH>::kThreads)
+    direct_worlds_kernel(const DirectWorld* __restrict__ worlds, const int3* __restrict__ tiles) {
+    __shared__ DirectWorld w;
+    const int3 t = tiles[blockIdx.x];
+    if (threadIdx.x == 0) w = worlds[t.x];
+    __syncthreads();
+    direct_tile<TW, TH, 1>(w.src, w.dst, w.weights, w.spans, w.g, w.p, t.y * TW, t.z * TH);
+}
+
+template <int TW, int TH, int NK>
 cudaError_t launch_t(const float* src, float* dst, const float* weights, const uint32_t* spans,
                      const DirectGeometry& g, const StepParams& p, cudaStream_t stream) {
     const int TP = TW + 2 * g.xp + 8;
@@ -174,6 +194,24 @@ cudaError_t launch_direct_step(int tile_cfg, int nk, const float* src, float* ds
     case kDirectTile64x32: return launch_nk<64, 32>(nk, src, dst, weights, spans, g, p, stream);
     default: return cudaErrorInvalidValue;
     }
+}
+
+cudaError_t launch_direct_worlds(const DirectWorld* worlds, const int3* tiles, int ntiles, int max_r,
+                                 cudaStream_t stream) {
+    // 32x16 tiles (small worlds); shared memory sized for the largest radius.
+    constexpr int TW = 32, TH = 16;
+    DirectGeometry g;
+    g.r = max_r;
+    g.ksize = 2 * max_r + 1;
+    g.xp = (max_r + 3) / 4 * 4;
+    g.wp = 2 * g.xp + 8;
+    const size_t smem = direct_smem_bytes(kDirectTile32x16, 1, g);
+    auto fn = direct_worlds_kernel<TW, TH>;
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) return e;
+    if (ntiles <= 0) return cudaSuccess;
+    fn<<<ntiles, DirectTile<TW, TH>::kThreads, smem, stream>>>(worlds, tiles);
+    return cudaGetLastError();
 }
 
 }  // namespace lenia

@@ -139,13 +139,15 @@ struct ColK {
 
 template <class PF, int B>
 __global__ void __launch_bounds__(ColK<PF, B>::T)
-    col_fast_kernel(const float2* __restrict__ S, float2* __restrict__ U, const float* __restrict__ khat,
-                    const float2* __restrict__ twf_g, const float2* __restrict__ twi_g, int M, int nk) {
+    col_fast_kernel(SpectralWorld w0, const SpectralWorld* __restrict__ worlds,
+                    const float2* __restrict__ twf_g, const float2* __restrict__ twi_g) {
     using K = ColK<PF, B>;
     using PI = typename K::PI;
     using IL = PassIdx<PF, PF::np - 1>;
     constexpr int H = K::H, T = K::T, PITCH = K::PITCH, RL = K::RL, NRL = K::NRL, Hh = K::Hh;
     extern __shared__ __align__(16) float2 sm[];
+    __shared__ SpectralWorld sw;  // this CTA's world
+    if (threadIdx.x == 0) sw = worlds ? worlds[blockIdx.y] : w0;
     float2* twf = sm;
     float2* twi = twf + PF::tw_size();
     float2* ba = twi + PI::tw_size();
@@ -154,6 +156,10 @@ __global__ void __launch_bounds__(ColK<PF, B>::T)
     copy_table(twf, twf_g, PF::tw_size());
     copy_table(twi, twi_g, PI::tw_size());
     __syncthreads();
+    const float2* __restrict__ S = sw.S;
+    float2* __restrict__ U = sw.U;
+    const float* __restrict__ khat = sw.khat;
+    const int M = sw.M, nk = sw.nk;
     for (int k0 = blockIdx.x * B; k0 < M; k0 += gridDim.x * B) {
         const int cols = min(B, M - k0);
         // Element (b, ky) of this group in the blocked layout.
@@ -246,15 +252,16 @@ struct RowK {
 // A into S_next (the first step after an upload or init).
 template <class PI, int RB>
 __global__ void __launch_bounds__(RowK<PI, RB>::T)
-    row_fast_kernel(const float2* __restrict__ U, const float* __restrict__ A, float* __restrict__ A_out,
-                    float2* __restrict__ S_next, const float2* __restrict__ twr_g,
-                    const float2* __restrict__ twi_g, const float2* __restrict__ twf_g, int H, int nk,
-                    StepParams p) {
+    row_fast_kernel(SpectralWorld w0, const SpectralWorld* __restrict__ worlds,
+                    const float2* __restrict__ twr_g, const float2* __restrict__ twi_g,
+                    const float2* __restrict__ twf_g) {
     using K = RowK<PI, RB>;
     using PF = typename K::PF;
     using IL = PassIdx<PI, PI::np - 1>;
     constexpr int M = K::M, W = 2 * M, T = K::T, PITCH = K::PITCH, RC = K::RC, NRC = K::NRC;
     extern __shared__ __align__(16) float2 sm[];
+    __shared__ SpectralWorld sw;  // this CTA's world
+    if (threadIdx.x == 0) sw = worlds ? worlds[blockIdx.y] : w0;
     float2* twr = sm;
     float2* twi = twr + (M + 1);
     float2* twf = twi + PI::tw_size();
@@ -263,6 +270,13 @@ __global__ void __launch_bounds__(RowK<PI, RB>::T)
     copy_table(twr, twr_g, M + 1);
     copy_table(twi, twi_g, PI::tw_size());
     copy_table(twf, twf_g, PF::tw_size());
+    __syncthreads();
+    const float2* __restrict__ U = sw.U;
+    const float* __restrict__ A = sw.A;
+    float* __restrict__ A_out = sw.A_out;
+    float2* __restrict__ S_next = sw.S_next;
+    const int H = int(sw.p.height), nk = sw.nk;
+    const StepParams& p = sw.p;
     const bool asym = p.growth_mode == 1u;
     const bool jitter = p.mu_jitter > 0.0f;
     for (int y0 = blockIdx.x * RB; y0 < H; y0 += gridDim.x * RB) {
@@ -434,9 +448,17 @@ cudaError_t prepare(F fn, size_t smem) {
     return cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
 }
 
+// Persistent grid over n worlds: grid.y = world, grid.x = CTAs per world
+// (the resident CTAs of the device shared out, at most one per group).
+dim3 world_grid(int per_sm, int groups, int n) {
+    const int resident = std::max(1, per_sm) * sms();
+    const int x = std::max(1, std::min(groups, (resident + n - 1) / n));
+    return dim3(unsigned(x), unsigned(n));
+}
+
 template <class PF, int B>
-cudaError_t launch_col_t(const FftGeometry& g, const FastTables& t, const float2* S, float2* U,
-                         cudaStream_t s) {
+cudaError_t launch_col_t(const SpectralWorld& w0, const SpectralWorld* worlds, int n, int M,
+                         const FastTables& t, cudaStream_t s) {
     using K = ColK<PF, B>;
     auto fn = col_fast_kernel<PF, B>;
     const size_t smem = K::smem();
@@ -445,15 +467,13 @@ cudaError_t launch_col_t(const FftGeometry& g, const FastTables& t, const float2
     if (e != cudaSuccess) return e;
     int per = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, K::T, smem);
-    const int groups = (g.M + B - 1) / B;
-    const int grid = std::max(1, std::min(groups, std::max(1, per) * sms()));
-    fn<<<grid, K::T, smem, s>>>(S, U, g.khat, t.col_twf, t.col_twi, g.M, g.nk);
+    fn<<<world_grid(per, (M + B - 1) / B, n), K::T, smem, s>>>(w0, worlds, t.col_twf, t.col_twi);
     return cudaGetLastError();
 }
 
 template <class PI, int RB>
-cudaError_t launch_row_t(const FftGeometry& g, const FastTables& t, const float2* U, const float* A,
-                         float* A_out, float2* S_next, const StepParams& p, int nk, cudaStream_t s) {
+cudaError_t launch_row_t(const SpectralWorld& w0, const SpectralWorld* worlds, int n, int H,
+                         const float2* tw_r2c, const FastTables& t, cudaStream_t s) {
     using K = RowK<PI, RB>;
     auto fn = row_fast_kernel<PI, RB>;
     const size_t smem = K::smem();
@@ -462,9 +482,7 @@ cudaError_t launch_row_t(const FftGeometry& g, const FastTables& t, const float2
     if (e != cudaSuccess) return e;
     int per = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, K::T, smem);
-    const int groups = (g.H + RB - 1) / RB;
-    const int grid = std::max(1, std::min(groups, std::max(1, per) * sms()));
-    fn<<<grid, K::T, smem, s>>>(U, A, A_out, S_next, g.tw_r2c, t.row_twi, t.row_twf, g.H, nk, p);
+    fn<<<world_grid(per, (H + RB - 1) / RB, n), K::T, smem, s>>>(w0, worlds, tw_r2c, t.row_twi, t.row_twf);
     return cudaGetLastError();
 }
 
@@ -528,33 +546,72 @@ void fast_plan_twiddles(const FastPlan& plan, std::vector<float2>& out) {
     }
 }
 
-cudaError_t launch_col_fast(const FftGeometry& g, const FastTables& t, int batch, const float2* S,
-                            float2* U, cudaStream_t s) {
-    switch (g.H) {
-#define X(n, ...)                                                             \
-    case n:                                                                   \
-        if (batch == 8) return launch_col_t<__VA_ARGS__, 8>(g, t, S, U, s);   \
-        if (batch == 4) return launch_col_t<__VA_ARGS__, 4>(g, t, S, U, s);   \
-        return launch_col_t<__VA_ARGS__, 2>(g, t, S, U, s);
+namespace {
+
+cudaError_t col_dispatch(int H, int M, int batch, const SpectralWorld& w0, const SpectralWorld* worlds, int n,
+                         const FastTables& t, cudaStream_t s) {
+    switch (H) {
+#define X(h, ...)                                                                       \
+    case h:                                                                             \
+        if (batch == 8) return launch_col_t<__VA_ARGS__, 8>(w0, worlds, n, M, t, s);    \
+        if (batch == 4) return launch_col_t<__VA_ARGS__, 4>(w0, worlds, n, M, t, s);    \
+        return launch_col_t<__VA_ARGS__, 2>(w0, worlds, n, M, t, s);
         LENIA_COL_PLANS(X)
 #undef X
     default: return cudaErrorNotSupported;
     }
 }
 
-cudaError_t launch_row_fast(const FftGeometry& g, const FastTables& t, int batch, const float2* U,
-                            const float* A, float* A_out, float2* S_next, const StepParams& p,
-                            int nk, cudaStream_t s) {
-    switch (g.M) {
-#define X(n, ...)                                                                                 \
-    case n:                                                                                       \
-        if (batch == 4) return launch_row_t<__VA_ARGS__, 4>(g, t, U, A, A_out, S_next, p, nk, s); \
-        if (batch == 2) return launch_row_t<__VA_ARGS__, 2>(g, t, U, A, A_out, S_next, p, nk, s); \
-        return launch_row_t<__VA_ARGS__, 1>(g, t, U, A, A_out, S_next, p, nk, s);
+cudaError_t row_dispatch(int H, int M, int batch, const SpectralWorld& w0, const SpectralWorld* worlds, int n,
+                         const float2* tw_r2c, const FastTables& t, cudaStream_t s) {
+    switch (M) {
+#define X(m, ...)                                                                                  \
+    case m:                                                                                        \
+        if (batch == 4) return launch_row_t<__VA_ARGS__, 4>(w0, worlds, n, H, tw_r2c, t, s);       \
+        if (batch == 2) return launch_row_t<__VA_ARGS__, 2>(w0, worlds, n, H, tw_r2c, t, s);       \
+        return launch_row_t<__VA_ARGS__, 1>(w0, worlds, n, H, tw_r2c, t, s);
         LENIA_ROW_PLANS(X)
 #undef X
     default: return cudaErrorNotSupported;
     }
+}
+
+}  // namespace
+
+cudaError_t launch_col_fast(const FftGeometry& g, const FastTables& t, int batch, const float2* S,
+                            float2* U, cudaStream_t s) {
+    SpectralWorld w{};
+    w.S = S;
+    w.U = U;
+    w.khat = g.khat;
+    w.M = g.M;
+    w.nk = g.nk;
+    return col_dispatch(g.H, g.M, batch, w, nullptr, 1, t, s);
+}
+
+cudaError_t launch_row_fast(const FftGeometry& g, const FastTables& t, int batch, const float2* U,
+                            const float* A, float* A_out, float2* S_next, const StepParams& p,
+                            int nk, cudaStream_t s) {
+    SpectralWorld w{};
+    w.U = const_cast<float2*>(U);  // read only by the row pass
+    w.A = A;
+    w.A_out = A_out;
+    w.S_next = S_next;
+    w.M = g.M;
+    w.nk = nk;
+    w.p = p;
+    w.p.height = uint32_t(g.H);
+    return row_dispatch(g.H, g.M, batch, w, nullptr, 1, g.tw_r2c, t, s);
+}
+
+cudaError_t launch_col_fast_worlds(int H, int M, const FastTables& t, int batch, const SpectralWorld* worlds,
+                                   int n, cudaStream_t s) {
+    return col_dispatch(H, M, batch, SpectralWorld{}, worlds, n, t, s);
+}
+
+cudaError_t launch_row_fast_worlds(int H, int M, const FastTables& t, const float2* tw_r2c, int batch,
+                                   const SpectralWorld* worlds, int n, cudaStream_t s) {
+    return row_dispatch(H, M, batch, SpectralWorld{}, worlds, n, tw_r2c, t, s);
 }
 
 }  // namespace lenia

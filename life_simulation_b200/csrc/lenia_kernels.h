@@ -22,6 +22,20 @@ struct DirectGeometry {
 };
 
 size_t direct_smem_bytes(int tile_cfg, int nk, const DirectGeometry& g);
+
+// One world of a batched direct launch (single kernel LUT). Its LUT uses the
+// world's own geometry g (radius r <= the launch's max_r).
+struct DirectWorld {
+    const float* src;
+    float* dst;
+    const float* weights;   // [2r+1][wp]
+    const uint32_t* spans;  // [2r+1]
+    DirectGeometry g;
+    StepParams p;
+};
+// tiles[i] = (world, tile x, tile y) of 32x16 output tiles.
+cudaError_t launch_direct_worlds(const DirectWorld* worlds, const int3* tiles, int ntiles, int max_r,
+                                 cudaStream_t stream);
 cudaError_t launch_direct_step(int tile_cfg, int nk, const float* src, float* dst,
                                const float* weights, const uint32_t* spans,
                                const DirectGeometry& g, const StepParams& p, cudaStream_t stream);
@@ -82,6 +96,20 @@ struct FastTables {
     const float2* row_twi = nullptr;  // row inverse plan
     const float2* row_twf = nullptr;  // row forward plan (reversed passes)
 };
+// One world of a spectral pass launch. A launch covers one world (passed by
+// value) or a table of worlds of the same size (blockIdx.y = world index).
+struct SpectralWorld {
+    const float2* S;     // row spectrum of A (blocked layout)
+    float2* U;           // nk potential spectra (blocked layout)
+    const float* khat;   // nk kernel spectra, (M+1) x (H/2+1) each
+    const float* A;      // state in
+    float* A_out;        // state out
+    float2* S_next;      // row spectrum of A_out, or null
+    int M;               // columns of the half spectrum (W/2)
+    int nk;              // kernels (0: row pass computes only S_next of A)
+    StepParams p;
+};
+
 bool fast_col_plan(int H, FastPlan& forward_plan);
 bool fast_row_plan(int M, FastPlan& inverse_plan);
 void fast_plan_twiddles(const FastPlan& plan, std::vector<float2>& out);
@@ -93,6 +121,13 @@ cudaError_t launch_col_fast(const FftGeometry& g, const FastTables& t, int batch
 cudaError_t launch_row_fast(const FftGeometry& g, const FastTables& t, int batch, const float2* U,
                             const float* A, float* A_out, float2* S_next, const StepParams& p,
                             int nk, cudaStream_t s);
+// Many worlds of one size (W = 2M, H) in one launch per pass: `worlds` is a
+// device array of n entries; H, M select the compile-time plans. tw_r2c:
+// exp(-2 pi i k / W), k <= M (device).
+cudaError_t launch_col_fast_worlds(int H, int M, const FastTables& t, int batch,
+                                   const SpectralWorld* worlds, int n, cudaStream_t s);
+cudaError_t launch_row_fast_worlds(int H, int M, const FastTables& t, const float2* tw_r2c, int batch,
+                                   const SpectralWorld* worlds, int n, cudaStream_t s);
 
 // ------------------------------------------------------------------ inits
 cudaError_t launch_init_noise(float* A, const InitParams& p, cudaStream_t s);

@@ -80,6 +80,31 @@ def fft3_params(w: int, h: int, conv: str = "fft") -> dict:
     }
 
 
+def sweep512(count_per_size: int = 128):
+    """The 512-world sweep: 128 worlds each of 128x128, 256x256, 384x216 and
+    512x512; per world (seed 3 + world id, SplitMix64) radius uniform in
+    8..32, mu in U[0.10, 0.35], sigma in U[0.01, 0.05], dt in U[0.05, 0.2];
+    single Gaussian-shell ring (shell sigma 0.15), growth mode 0; init
+    uniform[0,1) in a central square of side min(W, H)/4.
+    Returns (list of world parameter dicts, list of initial fields)."""
+    sizes = [(128, 128), (256, 256), (384, 216), (512, 512)]
+    worlds, inits = [], []
+    wid = 0
+    for (w, h) in sizes:
+        for _ in range(count_per_size):
+            u = uniform01(3 + wid, 5)
+            worlds.append({"width": w, "height": h, "radius": 8 + min(24, int(u[0] * 25)),
+                           "mu": 0.10 + 0.25 * float(u[1]), "sigma": 0.01 + 0.04 * float(u[2]),
+                           "dt": 0.05 + 0.15 * float(u[3]), "seed": 3 + wid})
+            side = min(w, h) // 4
+            a = np.zeros((h, w), np.float32)
+            y0, x0 = (h - side) // 2, (w - side) // 2
+            a[y0:y0 + side, x0:x0 + side] = uniform01(10_000 + wid, side * side).reshape(side, side)
+            inits.append(a)
+            wid += 1
+    return worlds, inits
+
+
 def workload(name: str):
     """(params, width, height, initial field) of a named workload."""
     if name == "single_256":
