@@ -291,6 +291,61 @@ int lenia_fft_step_noalloc(const float* field_in, float* field_out, uint32_t wid
 /* Message of the calling thread's last failed lenia_fft_step_noalloc. */
 const char* lenia_noalloc_last_message(void);
 
+/* ---- Gradient of a rollout (adjoint of the spectral step) ----
+ * No counterpart in the reference (it only steps forward). A batch of worlds
+ * of one size shares one set of kernels and growth parameters; each world has
+ * its own initial field. lenia_adjoint_forward runs T spectral steps of the
+ * reference's multi-kernel update (Lenia.metal:188-231 without noise, mu
+ * jitter or injection) from A_0 to A_T and keeps A every `checkpoint_every`
+ * steps; lenia_adjoint_backward takes dL/dA_T and returns dL/dA_0 and dL/d of
+ * every scalar parameter, recomputing each segment between checkpoints
+ * (checkpointed backpropagation through time). The backward of a step is
+ * hand-written: clip mask (subgradient 1 strictly inside (0, 1), 0 on or
+ * outside), growth derivative, and the adjoint convolution as spectrum
+ * products between forward and inverse FFTs.
+ *
+ * Kernels are built in FP64 ring by ring (buildRingKernelImage's formula,
+ * Lenia.cpp:95-125): K_k = sum_i beta_i R_i / sum_i beta_i sum(R_i).
+ * Sizes: the compile-time FFT sizes of the spectral path (height and width/2
+ * in 64, 128, 192(width only), 256, 512, 960(width only), 1024(height),
+ * 1080(height), 2048, 4096(height); e.g. 512x512, 1920x1080). */
+typedef struct lenia_adjoint_config {
+    uint32_t width, height;
+    uint32_t batch;             /* worlds */
+    uint32_t radius;            /* R (px); kernel k has radius R * radius_scale */
+    uint32_t kernel_core;       /* LENIA_CORE_* */
+    float shell_sigma;          /* Gaussian shell width (LENIA_CORE_GAUSS_SHELL) */
+    uint32_t growth_mode;       /* 0 standard, 1 asymptotic */
+    float dt;
+    uint32_t num_kernels;       /* 1..4 */
+    lenia_kernel_def kernels[4];
+    uint32_t steps;             /* T >= 1 */
+    uint32_t checkpoint_every;  /* 1..T */
+} lenia_adjoint_config;
+typedef struct lenia_adjoint lenia_adjoint;
+/* Parameter gradient layout (doubles): kernel k at k * 11 + {0: mu,
+ * 1: sigma, 2: weight, 3..10: betas[0..7]}, then dt at index 44. */
+#define LENIA_ADJOINT_PARAMS_PER_KERNEL 11
+#define LENIA_ADJOINT_NUM_PARAMS 45
+int lenia_adjoint_create(const lenia_adjoint_config* cfg, lenia_adjoint** out);
+int lenia_adjoint_destroy(lenia_adjoint* a);
+/* New parameter values (same num_kernels and num_betas per kernel; radius
+ * scales and the core stay). Takes effect for the next forward. */
+int lenia_adjoint_set_params(lenia_adjoint* a, const lenia_kernel_def* kernels, uint32_t num_kernels,
+                             float dt);
+/* a0: batch x height x width floats (device); a_final receives A_T (device).
+ * Asynchronous on `stream` (NULL: the context's stream). */
+int lenia_adjoint_forward(lenia_adjoint* a, const float* a0, float* a_final, void* stream);
+/* After lenia_adjoint_forward (same parameters): g_final = dL/dA_T (device,
+ * batch x height x width); g_initial receives dL/dA_0 (device, may alias
+ * g_final); grad_params, if not NULL, receives LENIA_ADJOINT_NUM_PARAMS
+ * doubles (device), summed over the batch. Asynchronous on `stream`. */
+int lenia_adjoint_backward(lenia_adjoint* a, const float* g_final, float* g_initial, double* grad_params,
+                           void* stream);
+/* Device memory held, and launches issued since creation. */
+int lenia_adjoint_stats(lenia_adjoint* a, uint64_t* device_bytes, uint64_t* launches);
+const char* lenia_adjoint_last_message(lenia_adjoint* a);
+
 /* Message of the last warning or error on this context ("" if none). */
 const char* lenia_last_message(lenia_ctx* ctx);
 const char* lenia_status_string(int status);

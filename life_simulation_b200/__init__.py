@@ -95,7 +95,21 @@ EXPORTS = (
     "lenia_batch_create", "lenia_batch_destroy", "lenia_batch_upload", "lenia_batch_download",
     "lenia_batch_step", "lenia_batch_stats", "lenia_batch_world_path", "lenia_batch_sync",
     "lenia_batch_last_message",
+    "lenia_adjoint_create", "lenia_adjoint_destroy", "lenia_adjoint_set_params",
+    "lenia_adjoint_forward", "lenia_adjoint_backward", "lenia_adjoint_stats",
+    "lenia_adjoint_last_message",
 )
+
+ADJOINT_PARAMS_PER_KERNEL = 11
+ADJOINT_NUM_PARAMS = 45
+
+
+class AdjointConfig(ctypes.Structure):
+    """lenia_adjoint_config (a batch of worlds for gradient computation)."""
+    _fields_ = [("width", ctypes.c_uint32), ("height", ctypes.c_uint32), ("batch", ctypes.c_uint32),
+                ("radius", ctypes.c_uint32), ("kernel_core", ctypes.c_uint32), ("shell_sigma", ctypes.c_float),
+                ("growth_mode", ctypes.c_uint32), ("dt", ctypes.c_float), ("num_kernels", ctypes.c_uint32),
+                ("kernels", KernelDef * 4), ("steps", ctypes.c_uint32), ("checkpoint_every", ctypes.c_uint32)]
 
 BATCH_AUTO, BATCH_DIRECT, BATCH_FFT = 0, 1, 2
 
@@ -169,6 +183,14 @@ def load_library(path: str = LIB_PATH):
     L.lenia_batch_sync.argtypes = [P]
     L.lenia_batch_last_message.argtypes = [P]
     L.lenia_batch_last_message.restype = ctypes.c_char_p
+    L.lenia_adjoint_create.argtypes = [ctypes.POINTER(AdjointConfig), pp]
+    L.lenia_adjoint_destroy.argtypes = [P]
+    L.lenia_adjoint_set_params.argtypes = [P, ctypes.POINTER(KernelDef), u32, ctypes.c_float]
+    L.lenia_adjoint_forward.argtypes = [P, P, P, P]
+    L.lenia_adjoint_backward.argtypes = [P, P, P, P, P]
+    L.lenia_adjoint_stats.argtypes = [P, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]
+    L.lenia_adjoint_last_message.argtypes = [P]
+    L.lenia_adjoint_last_message.restype = ctypes.c_char_p
     for name in EXPORTS:
         getattr(L, name)  # raises AttributeError if the build lacks a symbol
     _LIB = L
@@ -472,3 +494,112 @@ def single_world_params(w: World, conv: str) -> dict:
         p.update(convMode="fft", fftAnySize=True,
                  kernels=[{"radiusScale": 1.0, "mu": w.mu, "sigma": w.sigma, "weight": 1.0, "betas": [1.0]}])
     return p
+
+
+def kernel_defs(kernels) -> "ctypes.Array":
+    """lenia_kernel_def[4] from dicts with mu, sigma, weight, betas and an
+    optional radiusScale (the scene "kernels" entries)."""
+    arr = (KernelDef * 4)()
+    for i, k in enumerate(kernels):
+        d = arr[i]
+        d.radius_scale = float(k.get("radiusScale", 1.0))
+        d.mu, d.sigma, d.weight = float(k["mu"]), float(k["sigma"]), float(k.get("weight", 1.0))
+        betas = list(k.get("betas", [1.0]))
+        d.num_betas = len(betas)
+        for j, b in enumerate(betas):
+            d.betas[j] = float(b)
+    return arr
+
+
+CUDA_STREAM_LEGACY = 0x1  # cudaStreamLegacy
+
+
+def _stream_arg(stream: Optional[int]):
+    """None: the context's own stream (NULL); 0: the legacy default stream
+    (torch's default stream reports handle 0); else the handle."""
+    if stream is None:
+        return None
+    return ctypes.c_void_p(stream if stream else CUDA_STREAM_LEGACY)
+
+
+class LeniaAdjoint:
+    """Rollout and its gradient for a batch of worlds (lenia_adjoint_*).
+
+    Device buffers are passed as integer device pointers (e.g. a torch
+    tensor's data_ptr()): a0/a_final/g_final/g_initial hold batch x height x
+    width float32 values; grad_params LENIA_ADJOINT_NUM_PARAMS float64.
+    ``stream``: None queues on the context's own stream (ordered with
+    nothing else: synchronise before touching the buffers); an int handle
+    (0 = the legacy default stream, e.g. torch.cuda.current_stream()
+    .cuda_stream) orders the work with that stream."""
+
+    def __init__(self, width: int, height: int, batch: int, kernels, radius: int, steps: int,
+                 checkpoint_every: Optional[int] = None, dt: float = 0.1, growth_mode: int = 0,
+                 kernel_core: int = CORE_EXP, shell_sigma: float = 0.15):
+        if checkpoint_every is None:
+            checkpoint_every = min(8, steps)
+        L = load_library()
+        self._L = L
+        c = AdjointConfig()
+        c.width, c.height, c.batch, c.radius = width, height, batch, radius
+        c.kernel_core, c.shell_sigma, c.growth_mode, c.dt = kernel_core, shell_sigma, growth_mode, dt
+        c.num_kernels = len(kernels)
+        c.kernels = kernel_defs(kernels)
+        c.steps, c.checkpoint_every = steps, checkpoint_every
+        self.config = c
+        self.width, self.height, self.batch, self.steps = width, height, batch, steps
+        self.num_kernels = len(kernels)
+        self.num_betas = [len(k.get("betas", [1.0])) for k in kernels]
+        self.radius_scales = [float(k.get("radiusScale", 1.0)) for k in kernels]
+        self._h = ctypes.c_void_p()
+        rc = L.lenia_adjoint_create(ctypes.byref(c), ctypes.byref(self._h))
+        if rc < 0:
+            raise LeniaError(rc, L.lenia_adjoint_last_message(None).decode(errors="replace"))
+        self.forward_count = 0
+
+    def _check(self, rc: int) -> int:
+        if rc < 0:
+            raise LeniaError(rc, self._L.lenia_adjoint_last_message(self._h).decode(errors="replace"))
+        return rc
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            self._L.lenia_adjoint_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_params(self, kernels, dt: float) -> None:
+        kd = kernel_defs([dict(k, radiusScale=s) for k, s in zip(kernels, self.radius_scales)])
+        self._check(self._L.lenia_adjoint_set_params(self._h, kd, len(kernels), float(dt)))
+
+    def forward(self, a0_ptr: int, out_ptr: int, stream: Optional[int] = None) -> None:
+        self._check(self._L.lenia_adjoint_forward(self._h, ctypes.c_void_p(a0_ptr), ctypes.c_void_p(out_ptr),
+                                                  _stream_arg(stream)))
+        self.forward_count += 1
+
+    def backward(self, g_final_ptr: int, g_initial_ptr: int, grad_params_ptr: Optional[int] = None,
+                 stream: Optional[int] = None) -> None:
+        self._check(self._L.lenia_adjoint_backward(
+            self._h, ctypes.c_void_p(g_final_ptr), ctypes.c_void_p(g_initial_ptr),
+            ctypes.c_void_p(grad_params_ptr) if grad_params_ptr else None, _stream_arg(stream)))
+
+    def stats(self) -> dict:
+        b = ctypes.c_uint64()
+        n = ctypes.c_uint64()
+        self._check(self._L.lenia_adjoint_stats(self._h, ctypes.byref(b), ctypes.byref(n)))
+        return {"device_bytes": b.value, "launches": n.value}
+
+
+def unpack_param_grads(g: Sequence[float], num_betas: Sequence[int]) -> dict:
+    """The LENIA_ADJOINT_NUM_PARAMS gradient vector as per-kernel lists."""
+    K = len(num_betas)
+    per = ADJOINT_PARAMS_PER_KERNEL
+    return {"mu": [g[k * per] for k in range(K)], "sigma": [g[k * per + 1] for k in range(K)],
+            "weight": [g[k * per + 2] for k in range(K)],
+            "betas": [[g[k * per + 3 + j] for j in range(num_betas[k])] for k in range(K)],
+            "dt": g[ADJOINT_NUM_PARAMS - 1]}

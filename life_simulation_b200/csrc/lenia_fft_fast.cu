@@ -32,6 +32,7 @@
 #include <vector>
 
 #include "fft_ct.cuh"
+#include "fft_fast_common.cuh"
 #include "lenia_device.cuh"
 #include "lenia_kernels.h"
 
@@ -46,96 +47,9 @@ using namespace fftct;
 
 namespace {
 
-constexpr int KB = kSpectralBlock;  // columns per block of the blocked layout
-
-constexpr int roundup32(int x) { return (x + 31) / 32 * 32; }
-
-// Smallest pitch >= n with 2*pitch = 8 (mod 32) (in float2): transforms of a
-// batch start 8 banks apart.
-constexpr int row_pitch(int n) {
-    int p = n;
-    while ((2 * p) % 32 != 8) ++p;
-    return p;
-}
-
-// One Stockham pass over a batch of B transforms: item q -> (b = q % B,
-// j = q / B). All of a thread's items are loaded first, then twiddled,
-// transformed and stored. src(b, i) / dst(b, i, v) address element i of
-// transform b.
-template <class P, int PASS, bool INV, int B, int T, class Src, class Dst>
-__device__ __forceinline__ void pass_gen(Src&& src, Dst&& dst, const float2* __restrict__ tw, int cols) {
-    using I = PassIdx<P, PASS>;
-    constexpr int TOT = B * I::NR;
-    constexpr int ITEMS = (TOT + T - 1) / T;
-    float2 v[ITEMS][I::R];
-    int jj[ITEMS], bi[ITEMS];
-    bool ok[ITEMS];
-#pragma unroll
-    for (int it = 0; it < ITEMS; ++it) {
-        const int q = int(threadIdx.x) + it * T;
-        jj[it] = q / B;
-        bi[it] = q - jj[it] * B;
-        ok[it] = (TOT % T == 0 || q < TOT) && bi[it] < cols;
-        if (ok[it]) {
-#pragma unroll
-            for (int t = 0; t < I::R; ++t) v[it][t] = src(bi[it], I::in(jj[it], t));
-        }
-    }
-#pragma unroll
-    for (int it = 0; it < ITEMS; ++it) {
-        if (ok[it]) {
-            I::template twiddle<INV>(v[it], jj[it], tw);
-            Dft<I::R, INV>::run(v[it]);
-            const int ob = I::out_base(jj[it]);
-#pragma unroll
-            for (int t = 0; t < I::R; ++t) dst(bi[it], ob + t * I::NS, v[it][t]);
-        }
-    }
-}
-
-// Passes PASS..LAST-1 between two shared buffers (barrier after each);
-// returns the buffer that holds the data afterwards.
-template <class P, int PASS, int LAST, bool INV, int B, int T, int PITCH>
-__device__ __forceinline__ float2* mid_passes(float2* a, float2* b, const float2* __restrict__ tw, int cols) {
-    if constexpr (PASS < LAST) {
-        pass_gen<P, PASS, INV, B, T>([&](int bb, int i) { return a[bb * PITCH + i]; },
-                                     [&](int bb, int i, float2 v) { b[bb * PITCH + i] = v; }, tw, cols);
-        __syncthreads();
-        return mid_passes<P, PASS + 1, LAST, INV, B, T, PITCH>(b, a, tw, cols);
-    } else {
-        return a;
-    }
-}
-
-__device__ __forceinline__ void copy_table(float2* dst, const float2* __restrict__ src, int n) {
-    for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = __ldg(src + i);
-}
-
-// Asynchronous 16-byte global -> shared copy (completion: cp.async.wait_all,
-// a hardware wait, then a block barrier).
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+using namespace fastfft;
 
 // ------------------------------------------------------------- columns
-
-template <class PF, int B>
-struct ColK {
-    static_assert(KB % B == 0, "a column group lies inside one block");
-    using PI = typename Reverse<PF>::type;
-    static constexpr int H = PF::n;
-    static constexpr int Hh = H / 2 + 1;
-    static constexpr int RL = PF::last();
-    static constexpr int NRL = H / RL;
-    static constexpr int T = roundup32(B * NRL);
-    static constexpr int ITL = (B * NRL + T - 1) / T;
-    static constexpr int PITCH = row_pitch(H);
-    static constexpr size_t smem() {
-        return sizeof(float2) * (size_t(PF::tw_size()) + PI::tw_size() + 2 * size_t(B) * PITCH + H);
-    }
-};
 
 template <class PF, int B>
 __global__ void __launch_bounds__(ColK<PF, B>::T)
@@ -229,24 +143,6 @@ __global__ void __launch_bounds__(ColK<PF, B>::T)
 
 // ---------------------------------------------------------------- rows
 
-template <class PI, int RB>
-struct RowK {
-    using PF = typename Reverse<PI>::type;
-    static constexpr int M = PI::n;
-    static_assert(M % KB == 0, "row length must be a whole number of blocks");
-    static constexpr int RC = PI::last();
-    static constexpr int NRC = M / RC;
-    static constexpr int T = roundup32(RB * NRC);
-    static constexpr int ITL = (RB * NRC + T - 1) / T;
-    static constexpr int PITCH = row_pitch(M);  // even: rows start 16-byte aligned
-    // Twiddle tables, then the buffers from an even float2 offset so the
-    // 16-byte cp.async destinations are 16-byte aligned.
-    static constexpr int TABLES = (M + 1) + PI::tw_size() + PF::tw_size();
-    static constexpr int BUF0 = (TABLES + 1) / 2 * 2;
-    static_assert(PITCH % 2 == 0, "row pitch must keep 16-byte alignment");
-    static constexpr size_t smem() { return sizeof(float2) * (size_t(BUF0) + 2 * size_t(RB) * PITCH); }
-};
-
 // nk > 0: inverse row transforms of U_k, growth, A' (+ the next step's row
 // spectrum when S_next != null). nk == 0: only the forward row transform of
 // A into S_next (the first step after an upload or init).
@@ -294,31 +190,12 @@ __global__ void __launch_bounds__(RowK<PI, RB>::T)
         for (int kk = 0; kk < nk; ++kk) {
             // Stage rows y0..y0+rows of U_k: per block, rows x 8 columns are
             // contiguous (16-byte async copies, two columns each).
-            const float2* Uk = U + size_t(kk) * M * H;
-            for (int q = threadIdx.x; q < (M / KB) * RB * (KB / 2); q += T) {
-                const int c2 = q % (KB / 2);
-                const int b = (q / (KB / 2)) % RB;
-                const int kb = q / ((KB / 2) * RB);
-                if (b < rows)
-                    cp_async16(ba + b * PITCH + kb * KB + 2 * c2, Uk + (size_t(kb) * H + y0 + b) * KB + 2 * c2);
-            }
+            stage_rows<M, RB, T, PITCH>(ba, U + size_t(kk) * M * H, H, y0, rows);
             cp_async_wait_all();
             __syncthreads();
-            // Inverse of the real-FFT split folded into the first pass's loads:
-            // Z'[k] = (X[k] + conj X[M-k]) + i exp(+2 pi i k/W) (X[k] - conj X[M-k]).
-            pass_gen<PI, 0, true, RB, T>(
-                [&](int b, int i) {
-                    const float2* xr = ba + b * PITCH;
-                    if (i == 0) {
-                        const float2 x0 = xr[0];
-                        return make_float2(x0.x + x0.y, x0.x - x0.y);
-                    }
-                    const float2 Xk = xr[i];
-                    const float2 Xm = cconj(xr[M - i]);
-                    const float2 D = cmul(cconj(twr[i]), csub(Xk, Xm));
-                    return cadd(cadd(Xk, Xm), make_float2(-D.y, D.x));
-                },
-                [&](int b, int i, float2 v) { bb[b * PITCH + i] = v; }, twi, rows);
+            // Inverse of the real-FFT split folded into the first pass's loads.
+            pass_gen<PI, 0, true, RB, T>([&](int b, int i) { return c2r_split<M>(ba + b * PITCH, twr, i); },
+                                         [&](int b, int i, float2 v) { bb[b * PITCH + i] = v; }, twi, rows);
             __syncthreads();
             float2* X = mid_passes<PI, 1, PI::np - 1, true, RB, T, PITCH>(bb, ba, twi, rows);
             // Selects instead of a dynamic index into the parameter block (which
@@ -392,31 +269,7 @@ __global__ void __launch_bounds__(RowK<PI, RB>::T)
         pass_gen<PF, PF::np - 1, false, RB, T>([&](int b, int i) { return Y[b * PITCH + i]; },
                                                 [&](int b, int i, float2 v) { Zo[b * PITCH + i] = v; }, twf, rows);
         __syncthreads();
-        // Real-FFT split, stored into the blocked layout two columns at a time.
-        for (int q = threadIdx.x; q < (M / KB) * RB * (KB / 2); q += T) {
-            const int c2 = q % (KB / 2);
-            const int b = (q / (KB / 2)) % RB;
-            const int kb = q / ((KB / 2) * RB);
-            if (b >= rows) continue;
-            const float2* zr = Zo + b * PITCH;
-            float2 xv[2];
-#pragma unroll
-            for (int e = 0; e < 2; ++e) {
-                const int k = kb * KB + 2 * c2 + e;
-                const float2 Zk = zr[k];
-                if (k == 0) {
-                    xv[e] = make_float2(Zk.x + Zk.y, Zk.x - Zk.y);
-                } else {
-                    const float2 Zc = cconj(zr[M - k]);
-                    const float2 E = cscale(cadd(Zk, Zc), 0.5f);
-                    const float2 D = csub(Zk, Zc);
-                    const float2 O = make_float2(0.5f * D.y, -0.5f * D.x);
-                    xv[e] = cadd(E, cmul(twr[k], O));
-                }
-            }
-            *reinterpret_cast<float4*>(S_next + (size_t(kb) * H + y0 + b) * KB + 2 * c2) =
-                make_float4(xv[0].x, xv[0].y, xv[1].x, xv[1].y);
-        }
+        r2c_store_rows<M, RB, T, PITCH>(Zo, twr, S_next, H, y0, rows);
         __syncthreads();
     }
 }
@@ -428,32 +281,6 @@ void plan_radices(FastPlan& out) {
     out.n = P::n;
     out.np = P::np;
     for (int i = 0; i < P::np; ++i) out.radix[i] = P::radix(i);
-}
-
-int g_sms = 0;
-int sms() {
-    if (!g_sms) {
-        int d = 0;
-        cudaGetDevice(&d);
-        cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, d);
-        if (g_sms <= 0) g_sms = 148;
-    }
-    return g_sms;
-}
-
-template <typename F>
-cudaError_t prepare(F fn, size_t smem) {
-    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-    if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-}
-
-// Persistent grid over n worlds: grid.y = world, grid.x = CTAs per world
-// (the resident CTAs of the device shared out, at most one per group).
-dim3 world_grid(int per_sm, int groups, int n) {
-    const int resident = std::max(1, per_sm) * sms();
-    const int x = std::max(1, std::min(groups, (resident + n - 1) / n));
-    return dim3(unsigned(x), unsigned(n));
 }
 
 template <class PF, int B>
@@ -485,28 +312,6 @@ cudaError_t launch_row_t(const SpectralWorld& w0, const SpectralWorld* worlds, i
     fn<<<world_grid(per, (H + RB - 1) / RB, n), K::T, smem, s>>>(w0, worlds, tw_r2c, t.row_twi, t.row_twf);
     return cudaGetLastError();
 }
-
-// Column plans (forward order) by transform length. The last radix is
-// kept small: the column spectrum of the last pass lives in registers.
-#define LENIA_COL_PLANS(X)     \
-    X(1080, Plan<15, 9, 8>)    \
-    X(512, Plan<8, 8, 8>)      \
-    X(1024, Plan<16, 8, 8>)    \
-    X(4096, Plan<16, 16, 16>)  \
-    X(2048, Plan<16, 16, 8>)   \
-    X(256, Plan<16, 16>)       \
-    X(128, Plan<16, 8>)        \
-    X(216, Plan<6, 6, 6>)      \
-    X(64, Plan<8, 8>)
-// Row plans (inverse order) by M = W/2 (a multiple of 8).
-#define LENIA_ROW_PLANS(X)     \
-    X(960, Plan<8, 15, 8>)     \
-    X(512, Plan<8, 8, 8>)      \
-    X(2048, Plan<16, 8, 16>)   \
-    X(256, Plan<16, 16>)       \
-    X(192, Plan<8, 3, 8>)      \
-    X(128, Plan<16, 8>)        \
-    X(64, Plan<8, 8>)
 
 }  // namespace
 
@@ -544,6 +349,20 @@ void fast_plan_twiddles(const FastPlan& plan, std::vector<float2>& out) {
             }
         ns *= r;
     }
+}
+
+bool fast_twiddle_tables(int H, int M, std::vector<float2> (&out)[4]) {
+    FastPlan cf, ri;
+    if (!fast_col_plan(H, cf) || !fast_row_plan(M, ri)) return false;
+    FastPlan rcf = cf, rri = ri;
+    for (int i = 0; i < cf.np; ++i) rcf.radix[i] = cf.radix[cf.np - 1 - i];
+    for (int i = 0; i < ri.np; ++i) rri.radix[i] = ri.radix[ri.np - 1 - i];
+    const FastPlan* plans[4] = {&cf, &rcf, &ri, &rri};
+    for (int q = 0; q < 4; ++q) {
+        fast_plan_twiddles(*plans[q], out[q]);
+        if (out[q].empty()) out[q].push_back(make_float2(1.0f, 0.0f));
+    }
+    return true;
 }
 
 namespace {

@@ -113,6 +113,10 @@ struct SpectralWorld {
 bool fast_col_plan(int H, FastPlan& forward_plan);
 bool fast_row_plan(int M, FastPlan& inverse_plan);
 void fast_plan_twiddles(const FastPlan& plan, std::vector<float2>& out);
+// The four per-pass twiddle tables of a size's plans, in FastTables order
+// (column forward, column inverse, row inverse, row forward); false when H or
+// M has no compile-time plan.
+bool fast_twiddle_tables(int H, int M, std::vector<float2> (&out)[4]);
 // batch: columns per CTA iteration (2, 4 or 8) / rows per CTA iteration
 // (1, 2 or 4). launch_row_fast with nk = 0 computes only the row spectrum of
 // A into S_next (U, A_out unused).

@@ -141,13 +141,41 @@ void build_ring_image(uint32_t w, uint32_t h, float radius_k, float shell_sigma,
     }
 }
 
+// Ring by ring in FP64: the terms of buildRingKernelImage (Lenia.cpp:95-125)
+// with peak 1 each, unnormalised (the kernel is sum_i beta_i R_i over
+// sum_i beta_i sum(R_i)). The gradient form needs the rings separately.
+void ring_shells_f64(uint32_t w, uint32_t h, double radius_k, double shell_sigma, uint32_t nshell,
+                     uint32_t core, std::vector<std::vector<double>>& rings) {
+    rings.assign(nshell, std::vector<double>(size_t(w) * h, 0.0));
+    if (nshell == 0 || radius_k <= 0.0) return;
+    for (uint32_t y = 0; y < h; ++y) {
+        int dy = int(y);
+        if (dy > int(h / 2)) dy -= int(h);
+        for (uint32_t x = 0; x < w; ++x) {
+            int dx = int(x);
+            if (dx > int(w / 2)) dx -= int(w);
+            const double r = std::sqrt(double(dx) * dx + double(dy) * dy);
+            if (!(r > 0.0 && r <= radius_k)) continue;
+            const double u = r / radius_k * double(nshell);
+            const uint32_t i = std::min<uint32_t>(uint32_t(u), nshell - 1);
+            double v;
+            if (core == LENIA_CORE_EXP) {
+                v = exp_core(u - double(i));
+            } else {
+                const double t = (u - double(i) - 0.5) / (shell_sigma * double(nshell));
+                v = std::exp(-0.5 * t * t);
+            }
+            rings[i][size_t(y) * w + x] = v;
+        }
+    }
+}
+
 // The kernel image is real and even in x and y separately (it depends on
 // dx^2 + dy^2 over offsets that are symmetric on the torus), so its DFT is
-// real: K^(kx, ky) = sum K[y][x] cos(2 pi kx x / w) cos(2 pi ky y / h).
-// Evaluated in FP64 over the nonzero taps, separably, then divided by w*h
-// (the inverse transforms of the spectral path are unnormalised).
-void kernel_spectrum(const std::vector<float>& img, uint32_t w, uint32_t h,
-                     std::vector<float>& out) {
+// real: K^(kx, ky) = sum K[y][x] cos(2 pi kx x / w) cos(2 pi ky y / h),
+// evaluated in FP64 over the nonzero taps, separably.
+template <typename T>
+static void even_spectrum(const std::vector<T>& img, uint32_t w, uint32_t h, std::vector<double>& out) {
     const uint32_t M1 = w / 2 + 1, Hh = h / 2 + 1;
     std::vector<double> cw(w), ch(h);
     for (uint32_t m = 0; m < w; ++m) cw[m] = std::cos(2.0 * M_PI * double(m) / double(w));
@@ -157,7 +185,7 @@ void kernel_spectrum(const std::vector<float>& img, uint32_t w, uint32_t h,
     for (uint32_t y = 0; y < h; ++y) {
         std::vector<std::pair<uint32_t, double>> t;
         for (uint32_t x = 0; x < w; ++x)
-            if (img[size_t(y) * w + x] != 0.0f) t.emplace_back(x, double(img[size_t(y) * w + x]));
+            if (img[size_t(y) * w + x] != T(0)) t.emplace_back(x, double(img[size_t(y) * w + x]));
         if (!t.empty()) {
             rows.push_back(y);
             taps.push_back(std::move(t));
@@ -170,14 +198,28 @@ void kernel_spectrum(const std::vector<float>& img, uint32_t w, uint32_t h,
             for (const auto& t : taps[i]) s += t.second * cw[(uint64_t(kx) * t.first) % w];
             rowsum[i * M1 + kx] = s;
         }
-    out.assign(size_t(M1) * Hh, 0.0f);
-    const double norm = 1.0 / (double(w) * double(h));
+    out.assign(size_t(M1) * Hh, 0.0);
     for (uint32_t kx = 0; kx < M1; ++kx)
         for (uint32_t ky = 0; ky < Hh; ++ky) {
             double s = 0.0;
             for (size_t i = 0; i < rows.size(); ++i) s += rowsum[i * M1 + kx] * ch[(uint64_t(ky) * rows[i]) % h];
-            out[size_t(kx) * Hh + ky] = float(s * norm);
+            out[size_t(kx) * Hh + ky] = s;
         }
+}
+
+void even_spectrum_f64(const std::vector<double>& img, uint32_t w, uint32_t h, std::vector<double>& out) {
+    even_spectrum(img, w, h, out);
+}
+
+// Divided by w*h (the inverse transforms of the spectral path are
+// unnormalised) and rounded once.
+void kernel_spectrum(const std::vector<float>& img, uint32_t w, uint32_t h,
+                     std::vector<float>& out) {
+    std::vector<double> d;
+    even_spectrum(img, w, h, d);
+    const double norm = 1.0 / (double(w) * double(h));
+    out.resize(d.size());
+    for (size_t i = 0; i < d.size(); ++i) out[i] = float(d[i] * norm);
 }
 
 bool fft_plan(int n, FftPlan& plan) {

@@ -226,6 +226,12 @@ void fill_twiddles(int n, std::vector<float2>& tw);
 // out[kx * (h/2+1) + ky], kx <= w/2, ky <= h/2 (FP64, rounded once).
 void kernel_spectrum(const std::vector<float>& img, uint32_t w, uint32_t h,
                      std::vector<float>& out);
+// The same spectrum unnormalised and unrounded, of an FP64 image.
+void even_spectrum_f64(const std::vector<double>& img, uint32_t w, uint32_t h, std::vector<double>& out);
+// The rings of a kernel separately, FP64, peak 1 each, unnormalised
+// (buildRingKernelImage's terms, Lenia.cpp:95-125).
+void ring_shells_f64(uint32_t w, uint32_t h, double radius_k, double shell_sigma, uint32_t nshell,
+                     uint32_t core, std::vector<std::vector<double>>& rings);
 uint32_t pcg_hash_host(uint32_t v);
 uint32_t derive_seed(uint32_t global_seed, uint32_t tag);
 
