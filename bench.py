@@ -20,6 +20,10 @@ pixels x steps; ``value`` is whole-job Mpixel-steps/s.
   against the measured copy bandwidth in MEASURED_PEAKS.json.
 * cpu_baseline: the reference's own Lenia module and kernels compiled for
   the CPU (oracle/_ref), on a bounded row band of the same workload.
+* adjoint: the gradient form on 32 worlds of 512x512 (K=2, R=16, T=64,
+  checkpoints every 8): device time of the forward rollout and of the
+  backward (recomputation included), CUDA events on the launching stream
+  with an L2 flush before each; ratio = backward / forward.
 * --impl reference: that CPU reference alone, as the reference arm.
 """
 from __future__ import annotations
@@ -57,8 +61,11 @@ def parse_args():
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
-    ap.add_argument("--mode", choices=["step", "sweep"], default="step",
-                    help="step: the 1080p headline; sweep: the 512-world batched sweep")
+    ap.add_argument("--mode", choices=["step", "sweep", "adjoint"], default="step",
+                    help="step: the 1080p headline; sweep: the 512-world batched sweep; "
+                         "adjoint: the gradient form alone")
+    ap.add_argument("--adjoint-reps", type=int, default=5)
+    ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--plain-steps", type=int, default=10)
     return ap.parse_args()
 
@@ -338,6 +345,8 @@ def run_b200(args):
         "phases_ms_per_step": {k: v["ms"] / args.steps for k, v in phases.items()},
         "clocks": cl,
     })
+    if rank == 0 and world == 1 and not args.no_adjoint:
+        line["adjoint"] = adjoint_bench(args.adjoint_reps)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_baseline(params, w, h, init, args.cpu_seconds)
@@ -348,6 +357,73 @@ def run_b200(args):
     m.close()
     if world > 1:
         torch.distributed.destroy_process_group()
+    return 0
+
+
+def adjoint_bench(reps: int = 5, warmup: int = 3) -> dict:
+    """Forward rollout and backward of the gradient form on the adjoint_512
+    workload (life_simulation_b200/workloads.py), device-timed."""
+    import torch
+
+    import life_simulation_b200 as lb
+    from life_simulation_b200 import workloads as wl
+
+    c = wl.ADJOINT_512
+    B, W, H, T = c["batch"], c["width"], c["height"], c["steps"]
+    eng = lb.LeniaAdjoint(W, H, B, wl.ADJOINT_KERNELS, c["radius"], T, c["checkpoint_every"], c["dt"],
+                          c["growth_mode"], lb.CORE_EXP)
+    stream = torch.cuda.Stream()
+    sh = stream.cuda_stream
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    with torch.cuda.stream(stream):
+        a0 = torch.from_numpy(wl.adjoint_fields(4000, B, W, H)).cuda()
+        t0 = torch.from_numpy(wl.adjoint_fields(5000, B, W, H)).cuda()
+        target = torch.empty_like(t0)
+        eng.forward(t0.data_ptr(), target.data_ptr(), sh)
+        out = torch.empty_like(a0)
+        ga0 = torch.empty_like(a0)
+        gp = torch.empty(lb.ADJOINT_NUM_PARAMS, dtype=torch.float64, device="cuda")
+        fwd, bwd = [], []
+        for i in range(warmup + reps):
+            e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+            flush.zero_()
+            e[0].record(stream)
+            eng.forward(a0.data_ptr(), out.data_ptr(), sh)
+            e[1].record(stream)
+            g = 2.0 * (out - target) / out.numel()
+            flush.zero_()
+            e[2].record(stream)
+            eng.backward(g.data_ptr(), ga0.data_ptr(), gp.data_ptr(), sh)
+            e[3].record(stream)
+            stream.synchronize()
+            if i >= warmup:
+                fwd.append(e[0].elapsed_time(e[1]))
+                bwd.append(e[2].elapsed_time(e[3]))
+        loss = float(torch.mean((out - target) ** 2))
+        gnorm = float(ga0.abs().max())
+    st = eng.stats()
+    eng.close()
+    f, b = statistics.median(fwd), statistics.median(bwd)
+    px_steps = B * W * H * T
+    return {"workload": "adjoint_512: 32 worlds 512x512, K=2 R=16 b=[1],[0.5,1], T=64, checkpoints every 8",
+            "forward_ms": f, "backward_ms": b, "ratio": b / f,
+            "forward_mpx_steps_s": px_steps / (f / 1e3) / 1e6,
+            "backward_mpx_steps_s": px_steps / (b / 1e3) / 1e6,
+            "reps": reps, "loss": loss, "max_abs_grad_a0": gnorm,
+            "device_bytes": st["device_bytes"],
+            "timing": "median of reps; CUDA events on the launching stream; L2 flushed before each"}
+
+
+def run_adjoint(args):
+    import torch
+
+    torch.cuda.set_device(0)
+    r = adjoint_bench(args.adjoint_reps)
+    line = {"metric": "Lenia adjoint/forward time ratio (32 x 512x512, K=2, R=16, T=64, checkpoints every 8)",
+            "value": r["ratio"], "unit": "x", "higher_is_better": False, "n_gpus": 1, "dtype": "f32",
+            "data": "synthetic", "config": {"workload": r["workload"]}}
+    line.update(r)
+    print(json.dumps(line))
     return 0
 
 
@@ -424,6 +500,8 @@ def main():
         return run_reference(args)
     if args.mode == "sweep":
         return run_sweep(args)
+    if args.mode == "adjoint":
+        return run_adjoint(args)
     return run_b200(args)
 
 

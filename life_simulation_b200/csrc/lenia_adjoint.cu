@@ -203,7 +203,8 @@ __global__ void __launch_bounds__(RowK<PI, RB>::T)
                 *reinterpret_cast<float2*>(sw.g_out + gidx(it, t)) = gv[it][t];
             }
         }
-        float acc[ITL][RC][2];  // mode 0: sum_k h_k (2 b_k - 1); mode 1: sum_k h_k b_k
+        // The dt and mode-1 terms are linear in the kernels' contributions,
+        // so they are summed kernel by kernel (no per-pixel accumulator).
         for (int kk = 0; kk < nk; ++kk) {
             stage_rows<M, RB, T, PITCH>(ba, sw.U + size_t(kk) * M * H, H, y0, rows);
             cp_async_wait_all();
@@ -239,15 +240,16 @@ __global__ void __launch_bounds__(RowK<PI, RB>::T)
                         const float q = g * coef * b * dmu * inv_sigma;
                         pmu -= q;
                         psig += q * dmu;
-                        float c;
                         if (asym) {
+                            // dpre/dh_k = dt (b_k - G) / sum h; dpre/ddt = G - A_t.
+                            const float gb = sw_ok ? g * hw * b * inv_sw : 0.0f;
                             ph += sw_ok ? g * dt * b * inv_sw : 0.0f;
-                            c = hw * b;
+                            pdt += gb;
+                            pcommon += dt * inv_sw * gb;
                         } else {
                             ph += g * dt * (2.0f * b - 1.0f);
-                            c = hw * (2.0f * b - 1.0f);
+                            pdt += g * hw * (2.0f * b - 1.0f);
                         }
-                        acc[it][t][e] = kk == 0 ? c : acc[it][t][e] + c;
                         qv[e] = q;
                     }
                     zq[it][t] = make_float2(qv[0], qv[1]);
@@ -275,20 +277,15 @@ __global__ void __launch_bounds__(RowK<PI, RB>::T)
             r2c_store_rows<M, RB, T, PITCH>(Zo, twr, sw.SQ + size_t(kk) * M * H, H, y0, rows);
             __syncthreads();
         }
-        // dpre/ddt: mode 0 sum_k h_k (2 b_k - 1); mode 1 G - A_t.
+        // Mode 1's dt term: the -A_t part.
+        if (asym && sw_ok) {
 #pragma unroll
-        for (int it = 0; it < ITL; ++it) {
-            if (!ok[it]) continue;
+            for (int it = 0; it < ITL; ++it) {
+                if (!ok[it]) continue;
 #pragma unroll
-            for (int t = 0; t < RC; ++t) {
-                if (asym) {
-                    if (!sw_ok) continue;
+                for (int t = 0; t < RC; ++t) {
                     const float2 ac = __ldg(reinterpret_cast<const float2*>(sw.A_cur + gidx(it, t)));
-                    const float G0 = acc[it][t][0] * inv_sw, G1 = acc[it][t][1] * inv_sw;
-                    pdt += gv[it][t].x * (G0 - ac.x) + gv[it][t].y * (G1 - ac.y);
-                    pcommon += dt * inv_sw * (gv[it][t].x * G0 + gv[it][t].y * G1);
-                } else {
-                    pdt += gv[it][t].x * acc[it][t][0] + gv[it][t].y * acc[it][t][1];
+                    pdt -= gv[it][t].x * ac.x + gv[it][t].y * ac.y;
                 }
             }
         }
@@ -804,6 +801,66 @@ cudaError_t row_spectrum(lenia_adjoint* a, int j, cudaStream_t s) {
                                          a->nb, s);
 }
 
+// Columns per CTA iteration of the forward column pass and rows of the row
+// pass: each candidate timed (CUDA events, after one warm-up launch) on step
+// 0's tables over zeroed buffers; the fastest is kept.
+cudaError_t autotune(lenia_adjoint* a) {
+    const cudaStream_t s = a->stream;
+    cudaError_t e = cudaMemsetAsync(a->ckpt, 0, sizeof(float) * a->nb * a->P, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(a->Sring, 0, sizeof(float2) * a->nb * a->SPX, s);
+    if (e != cudaSuccess) return e;
+    cudaEvent_t t0, t1;
+    cudaEventCreate(&t0);
+    cudaEventCreate(&t1);
+    const auto timed = [&](auto launch, float* ms) -> cudaError_t {
+        cudaError_t r = launch();
+        if (r != cudaSuccess) return r;
+        cudaEventRecord(t0, s);
+        for (int i = 0; i < 3 && r == cudaSuccess; ++i) r = launch();
+        cudaEventRecord(t1, s);
+        if (r == cudaSuccess) r = cudaEventSynchronize(t1);
+        if (r == cudaSuccess) r = cudaEventElapsedTime(ms, t0, t1);
+        return r;
+    };
+    float best = 1e30f;
+    for (int cb : {8, 4, 2}) {
+        float ms = 0.0f;
+        const cudaError_t r = timed([&] {
+            return lenia::launch_col_fast_worlds(a->H, a->M, a->ft, cb, a->d_fcol, a->nb, s);
+        }, &ms);
+        if (r == cudaErrorInvalidConfiguration) continue;  // candidate too large for this size
+        if (r != cudaSuccess) {
+            e = r;
+            break;
+        }
+        if (ms < best) {
+            best = ms;
+            a->col_batch = cb;
+        }
+    }
+    best = 1e30f;
+    for (int rb : {4, 2, 1}) {
+        if (e != cudaSuccess) break;
+        float ms = 0.0f;
+        const cudaError_t r = timed([&] {
+            return lenia::launch_row_fast_worlds(a->H, a->M, a->ft, a->tw_r2c, rb, a->d_frow, a->nb, s);
+        }, &ms);
+        if (r == cudaErrorInvalidConfiguration) continue;
+        if (r != cudaSuccess) {
+            e = r;
+            break;
+        }
+        if (ms < best) {
+            best = ms;
+            a->row_batch = rb;
+        }
+    }
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    cudaGetLastError();
+    return e;
+}
+
 }  // namespace
 
 extern "C" {
@@ -884,6 +941,7 @@ int lenia_adjoint_create(const lenia_adjoint_config* cfg, lenia_adjoint** out) {
     a->ft.row_twf = a->tw[3];
     int rc = a->set_kernels(cfg->kernels, cfg->num_kernels, cfg->dt);
     if (rc != LENIA_OK) return bail(rc);
+    if ((e = autotune(a)) != cudaSuccess) return bail(a->cuda_fail(e, "autotune"));
     if ((e = cudaDeviceSynchronize()) != cudaSuccess) return bail(a->cuda_fail(e, "setup"));
     *out = a;
     return LENIA_OK;

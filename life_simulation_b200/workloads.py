@@ -7,6 +7,12 @@ from a seed by SplitMix64 (the algorithm of LifeCore/Math/Random.h:11-31,
 * ``single_256``: a 256x256 torus, direct convolution, R=13, exponential
   kernel core, growth mode 0 (mu 0.15, sigma 0.015, dt 0.1); uniform[0,1)
   in the central 64x64 square (seed 1), zeros elsewhere.
+* ``adjoint_512`` (the gradient form): 32 worlds of 512x512, two kernels
+  R=16, peaks [1] and [0.5, 1], mu {0.15, 0.25}, sigma {0.015, 0.03},
+  weights {0.5, 0.5}, dt 0.1, growth mode 0, exponential core, T=64 steps
+  with checkpoints every 8; world b starts from uniform[0,1) over the whole
+  field (SplitMix64 seed 4000 + b) and its target is the T-step state from
+  seed 5000 + b; loss = mean squared error over every world and pixel.
 * ``fft3_1080p`` / ``fft3_1024x512``: three kernels of radius 24, peaks
   [1], [0.5, 1], [1, 0.667, 0.333], mu {0.156, 0.193, 0.342}, sigma
   {0.0118, 0.049, 0.0891}, weights {0.5, 0.3, 0.2}, dt 0.1, growth mode 0,
@@ -78,6 +84,19 @@ def fft3_params(w: int, h: int, conv: str = "fft") -> dict:
         "kernelCore": "exp", "growthMode": 0, "dt": 0.1, "noiseAmount": 0.0, "muJitter": 0.0,
         "injectAmount": 0.0, "kernels": copy.deepcopy(FFT3_KERNELS),
     }
+
+
+ADJOINT_KERNELS = [
+    {"mu": 0.15, "sigma": 0.015, "weight": 0.5, "betas": [1.0]},
+    {"mu": 0.25, "sigma": 0.03, "weight": 0.5, "betas": [0.5, 1.0]},
+]
+ADJOINT_512 = {"width": 512, "height": 512, "batch": 32, "radius": 16, "steps": 64,
+               "checkpoint_every": 8, "dt": 0.1, "growth_mode": 0}
+
+
+def adjoint_fields(seed_base: int, batch: int = 32, w: int = 512, h: int = 512) -> np.ndarray:
+    """batch x h x w uniform[0,1) fields, world b from SplitMix64(seed_base + b)."""
+    return np.stack([uniform01(seed_base + b, w * h).reshape(h, w) for b in range(batch)])
 
 
 def sweep512(count_per_size: int = 128):
