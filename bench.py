@@ -24,6 +24,10 @@ pixels x steps; ``value`` is whole-job Mpixel-steps/s.
   checkpoints every 8): device time of the forward rollout and of the
   backward (recomputation included), CUDA events on the launching stream
   with an L2 flush before each; ratio = backward / forward.
+* tc: 4096x4096, 3 kernels R=32, 64 steps per arithmetic of the column DFT
+  stages (fp32 CUDA cores, fp16x3 / bf16x3 split-precision tensor cores);
+  per-step device time, the column pass's HBM roofline and tensor FLOP rate
+  (a radix-16 stage as a real 32x32 GEMM: 128 FLOP per point, x3 hi/lo).
 * --impl reference: that CPU reference alone, as the reference arm.
 """
 from __future__ import annotations
@@ -61,9 +65,10 @@ def parse_args():
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
-    ap.add_argument("--mode", choices=["step", "sweep", "adjoint"], default="step",
+    ap.add_argument("--mode", choices=["step", "sweep", "adjoint", "tc"], default="step",
                     help="step: the 1080p headline; sweep: the 512-world batched sweep; "
-                         "adjoint: the gradient form alone")
+                         "adjoint: the gradient form alone; tc: 4096^2 with the column DFT stages "
+                         "on FP32 CUDA cores vs split-precision tensor cores")
     ap.add_argument("--adjoint-reps", type=int, default=5)
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--plain-steps", type=int, default=10)
@@ -427,6 +432,73 @@ def run_adjoint(args):
     return 0
 
 
+def run_tc(args):
+    """the column DFT stages on the CUDA cores (FP32) and
+    on the tensor cores (FP16 / BF16 hi/lo, FP32 accumulation)."""
+    import torch
+
+    import life_simulation_b200 as lb
+    from life_simulation_b200 import workloads as wl
+
+    torch.cuda.set_device(0)
+    w = h = 4096
+    K, steps = 3, 64
+    init = wl.patches(w, h, 40, 256, seed=2)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    sh = stream.cuda_stream
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    peak, peak_kind = measured_peaks()
+    col_bytes = (4 + 2 * K + 4 * K) * w * h
+    # (1 forward + K inverse) column transforms x 3 radix-16 stages x H points
+    # x 128 FLOP (real 32x32 GEMM per 16 points) x 3 (hi/lo), per column.
+    tc_flops = (1 + K) * 3 * h * 128 * 3 * (w // 2)
+    res = {}
+    for prec in ("fp32", "fp16x3", "bf16x3"):
+        p = wl.fft3_params(w, h)
+        p["radius"] = 32
+        p["fftPrecision"] = prec
+        m = lb.LeniaModule(p, w, h)
+        m.reset(2)
+        m.upload(init)
+        fp = m.frame_params(0)
+        for i in range(max(3, args.warmup)):
+            fp.frame_index = fp.audio_frame = i
+            m.step(fp, 1, sh)
+        torch.cuda.synchronize()
+        m.profile(True)
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        for i in range(steps):
+            flush.zero_()
+            fp.frame_index = fp.audio_frame = 100 + i
+            evs[i][0].record(stream)
+            m.step(fp, 1, sh)
+            evs[i][1].record(stream)
+        torch.cuda.synchronize()
+        prof = m.profile_read()
+        m.profile(False)
+        step_ms = sum(a.elapsed_time(b) for a, b in evs) / steps
+        col = prof["column"]
+        col_ms = col["ms"] / col["count"]
+        r = {"ms_per_step": step_ms, "mpx_steps_s": w * h / (step_ms / 1e3) / 1e6,
+             "column_ms": col_ms, "row_ms": prof["row_growth"]["ms"] / prof["row_growth"]["count"],
+             "column_gbs": col_bytes / (col_ms / 1e3) / 1e9, "column_frac_hbm": col_bytes / (col_ms / 1e3) / 1e9 / peak,
+             "fft_precision": m.info()["fft_precision"]}
+        if prec != "fp32":
+            r["column_tensor_tflops"] = tc_flops / (col_ms / 1e3) / 1e12
+        res[prec] = r
+        m.close()
+    print(json.dumps({
+        "metric": "Lenia Mpixel-steps/s, 4096x4096 K=3 R=32: column DFT stages FP32 CUDA cores vs split-precision tensor cores",
+        "unit": UNIT, "value": res["fp32"]["mpx_steps_s"], "higher_is_better": True, "n_gpus": 1, "steps": steps,
+        "dtype": "f32 / fp16x3 / bf16x3", "data": "synthetic",
+        "config": {"workload": "4096x4096, 3 kernels R=32 (fft3 peaks/mu/sigma/h), 40 patches of 256x256 (seed 2)",
+                   "l2": "256 MiB write between steps"},
+        "peak_hbm_gbs": peak, "peak_source": peak_kind, "column_bytes_per_launch": col_bytes,
+        "column_tensor_flops_per_launch": tc_flops, "precisions": res}))
+    return 0
+
+
 def run_sweep(args):
     """512 worlds of mixed sizes, 240 substeps with the
     activity readback every 60, batched (one graph per 60 substeps) against
@@ -502,6 +574,8 @@ def main():
         return run_sweep(args)
     if args.mode == "adjoint":
         return run_adjoint(args)
+    if args.mode == "tc":
+        return run_tc(args)
     return run_b200(args)
 
 

@@ -92,7 +92,15 @@ typedef struct lenia_config {
     uint32_t stamp_count;          /* stampCount (6, max 32) */
     uint32_t stamp_rotate;         /* stampRotate (1) */
     uint32_t use_organism_params;  /* useOrganismParams (1) */
+    /* fftPrecision: arithmetic of the spectral path's column DFT stages.
+     * LENIA_FFT_FP32 (default): FP32 on the CUDA cores. LENIA_FFT_BF16X3 /
+     * LENIA_FFT_FP16X3: on the tensor cores with split-precision BF16 / FP16
+     * hi/lo operands and FP32 accumulation, for column lengths 256 and 4096
+     * (other sizes fall back to FP32 with a warning). No counterpart in the
+     * reference. */
+    uint32_t fft_precision;
 } lenia_config;
+enum { LENIA_FFT_FP32 = 0, LENIA_FFT_BF16X3 = 1, LENIA_FFT_FP16X3 = 2 };
 
 /* Per-frame values the reference reads through param(ctx, key, fallback)
  * (Lenia.cpp:456-464) plus the frame's indices. */
@@ -118,6 +126,7 @@ typedef struct lenia_info {
     uint32_t use_stamp_init;
     uint64_t device_bytes;    /* device memory held by the context */
     uint32_t fft_radix_row[8], fft_radix_col[8]; /* FFT plans (0-terminated) */
+    uint32_t fft_precision;   /* LENIA_FFT_* of the column DFT stages in use */
 } lenia_info;
 
 typedef struct lenia_ctx lenia_ctx;

@@ -31,6 +31,7 @@ LENIA_OK = 0
 LENIA_WARN_FALLBACK = 1
 CONV_DIRECT, CONV_FFT, CONV_DIRECT_MULTI = 0, 1, 2
 CORE_GAUSS_SHELL, CORE_EXP = 0, 1
+FFT_FP32, FFT_BF16X3, FFT_FP16X3 = 0, 1, 2
 INIT_NOISE, INIT_STAMP = 0, 1
 
 
@@ -61,7 +62,7 @@ class Config(ctypes.Structure):
                 ("org_R", ctypes.c_float), ("org_T", ctypes.c_float),
                 ("org_mu", ctypes.c_float), ("org_sigma", ctypes.c_float),
                 ("stamp_count", ctypes.c_uint32), ("stamp_rotate", ctypes.c_uint32),
-                ("use_organism_params", ctypes.c_uint32)]
+                ("use_organism_params", ctypes.c_uint32), ("fft_precision", ctypes.c_uint32)]
 
 
 class FrameParams(ctypes.Structure):
@@ -78,7 +79,7 @@ class Info(ctypes.Structure):
                 ("conv_mode", ctypes.c_uint32), ("radius", ctypes.c_uint32),
                 ("num_kernels", ctypes.c_uint32), ("use_stamp_init", ctypes.c_uint32),
                 ("device_bytes", ctypes.c_uint64), ("fft_radix_row", ctypes.c_uint32 * 8),
-                ("fft_radix_col", ctypes.c_uint32 * 8)]
+                ("fft_radix_col", ctypes.c_uint32 * 8), ("fft_precision", ctypes.c_uint32)]
 
 
 # Every symbol include/lenia_b200.h declares (checked by the CPU tests).
@@ -210,6 +211,7 @@ def config_from_params(params: dict) -> Config:
     c.sim_height = int(params.get("simHeight", 0))
     c.conv_mode = {"fft": CONV_FFT, "directMulti": CONV_DIRECT_MULTI}.get(params.get("convMode", "direct"), CONV_DIRECT)
     c.fft_any_size = int(bool(params.get("fftAnySize", False)))
+    c.fft_precision = {"fp32": FFT_FP32, "bf16x3": FFT_BF16X3, "fp16x3": FFT_FP16X3}[params.get("fftPrecision", "fp32")]
     if "radius" in params:
         c.has_radius, c.radius = 1, int(params["radius"])
     ks = params.get("kernels") or []
@@ -379,7 +381,7 @@ class LeniaModule:
                 "radius": i.radius, "num_kernels": i.num_kernels, "use_stamp_init": i.use_stamp_init,
                 "device_bytes": i.device_bytes,
                 "fft_radix_row": [r for r in i.fft_radix_row if r],
-                "fft_radix_col": [r for r in i.fft_radix_col if r]}
+                "fft_radix_col": [r for r in i.fft_radix_col if r], "fft_precision": i.fft_precision}
 
 
 def inspect(params, scene_w: int, scene_h: int, base_dir: Optional[str] = None) -> dict:

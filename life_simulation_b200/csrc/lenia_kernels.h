@@ -133,6 +133,14 @@ cudaError_t launch_col_fast_worlds(int H, int M, const FastTables& t, int batch,
 cudaError_t launch_row_fast_worlds(int H, int M, const FastTables& t, const float2* tw_r2c, int batch,
                                    const SpectralWorld* worlds, int n, cudaStream_t s);
 
+// Column pass with its DFT stages on the tensor cores (lenia_fft_tc.cu), same
+// contract and layout as launch_col_fast: precision 1 = BF16 hi/lo, 2 = FP16
+// hi/lo operands (FP32 accumulation); H with an all-radix-16 plan (256, 4096);
+// batch = columns per CTA iteration (256: 2/4/8, 4096: 1/2).
+bool tc_col_plan(int H);
+cudaError_t launch_col_tc(const FftGeometry& g, const FastTables& t, int precision, int batch, const float2* S,
+                          float2* U, cudaStream_t s);
+
 // ------------------------------------------------------------------ inits
 cudaError_t launch_init_noise(float* A, const InitParams& p, cudaStream_t s);
 cudaError_t launch_init_stamp(float* A, uint32_t w, uint32_t h, const float* org, uint32_t ow,

@@ -319,6 +319,15 @@ int config_from_json(const Json& p, const std::string& base_dir, ModuleConfig& c
                   : conv == "directMulti" ? LENIA_CONV_DIRECT_MULTI
                                           : LENIA_CONV_DIRECT;
     c.fft_any_size = p.value_bool("fftAnySize", false);
+    const std::string prec = p.value_string("fftPrecision", "fp32");
+    if (prec == "bf16x3") {
+        c.fft_precision = LENIA_FFT_BF16X3;
+    } else if (prec == "fp16x3") {
+        c.fft_precision = LENIA_FFT_FP16X3;
+    } else if (prec != "fp32") {
+        c.warnings.push_back("\"fftPrecision\" must be \"fp32\", \"bf16x3\" or \"fp16x3\" (got \"" + prec +
+                             "\"); using \"fp32\"");
+    }
     if (p.contains("radius")) {
         c.has_radius = true;
         c.radius = p.value_u32("radius", 13u);
@@ -382,6 +391,11 @@ int config_from_struct(const lenia_config& s, ModuleConfig& c, std::string& erro
     }
     c.conv_mode = s.conv_mode;
     c.fft_any_size = s.fft_any_size != 0;
+    if (s.fft_precision > LENIA_FFT_FP16X3) {
+        error = "fft_precision out of range";
+        return LENIA_ERR_INVALID_ARG;
+    }
+    c.fft_precision = s.fft_precision;
     c.has_radius = s.has_radius != 0;
     c.radius = s.radius;
     uint32_t nk = s.num_kernels;
@@ -535,6 +549,20 @@ int LeniaModule::resolve(uint32_t scene_w, uint32_t scene_h) {
                            " needs an even width and sizes with factors 2, 3, 5 only; falling back "
                            "to convMode=\"direct\"");
             use_fft_ = false;
+        }
+    }
+    // fftPrecision (extension): tensor-core column stages where the column
+    // plan is all radix 16 and the compile-time-plan passes run.
+    tc_precision_ = LENIA_FFT_FP32;
+    if (cfg_.fft_precision != LENIA_FFT_FP32) {
+        FastPlan cf, ri;
+        const bool ok = use_fft_ && w_ % 2 == 0 && (w_ / 2) % kSpectralBlock == 0 && tc_col_plan(int(h_)) &&
+                        fast_col_plan(int(h_), cf) && fast_row_plan(int(w_ / 2), ri);
+        if (ok) {
+            tc_precision_ = cfg_.fft_precision;
+        } else {
+            warn.push_back("\"fftPrecision\" on the tensor cores needs convMode=\"fft\" with simHeight 256 or 4096 "
+                           "(got " + std::to_string(w_) + "x" + std::to_string(h_) + "); using \"fp32\"");
         }
     }
     const bool multi = use_fft_ || direct_multi_;
@@ -842,6 +870,14 @@ int LeniaModule::autotuneSpectral() {
         });
         if (t < 0.97f * best_row) { best_row = t; row_batch_ = c; }
     }
+    if (tc_precision_ != LENIA_FFT_FP32) {
+        float best_tc = 1e30f;
+        for (int c : {8, 4, 2, 1}) {
+            const float t = time_it([&] { return launch_col_tc(fgeo_, fast_, int(tc_precision_), c, d_S_, d_U_, stream_); });
+            if (t < 0.97f * best_tc) { best_tc = t; tc_batch_ = c; }
+        }
+        if (best_tc >= 1e29f) tc_precision_ = LENIA_FFT_FP32;
+    }
     if (best_col >= 1e29f || best_row >= 1e29f) fast_col_ = fast_row_ = false;
     cudaGetLastError();
     event_pool_.push_back(a);
@@ -1036,6 +1072,8 @@ int LeniaModule::step(const lenia_frame_params& fp, uint32_t substeps, cudaStrea
                 if (e != cudaSuccess) return cudaFail(e, "row pass");
             }
             e = launch(LENIA_PHASE_COLUMN, s, [&] {
+                if (tc_precision_ != LENIA_FFT_FP32)
+                    return launch_col_tc(fgeo_, fast_, int(tc_precision_), tc_batch_, d_S_, d_U_, s);
                 return fast_col_ ? launch_col_fast(fgeo_, fast_, col_batch_, d_S_, d_U_, s)
                                  : launch_col_conv(fgeo_, d_S_, d_U_, s);
             });
@@ -1066,6 +1104,7 @@ void LeniaModule::info(lenia_info* o) const {
     o->num_kernels = num_k_;
     o->use_stamp_init = use_stamp_ ? 1u : 0u;
     o->device_bytes = device_bytes_;
+    o->fft_precision = tc_precision_;
     if (use_fft_) {
         for (int i = 0; i < fgeo_.row.npass && i < 8; ++i) o->fft_radix_row[i] = uint32_t(fgeo_.row.radix[i]);
         for (int i = 0; i < fgeo_.col.npass && i < 8; ++i) o->fft_radix_col[i] = uint32_t(fgeo_.col.radix[i]);

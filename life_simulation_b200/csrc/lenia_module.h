@@ -63,6 +63,7 @@ struct ModuleConfig {
     uint32_t sim_width = 0, sim_height = 0;
     uint32_t conv_mode = LENIA_CONV_DIRECT;
     bool fft_any_size = false;
+    uint32_t fft_precision = LENIA_FFT_FP32;  // fftPrecision (extension)
     bool has_radius = false;
     uint32_t radius = 13;
     bool has_kernels = false;
@@ -195,6 +196,8 @@ private:
     FftGeometry fgeo_{};
     bool fast_col_ = false, fast_row_ = false;  // compile-time-plan passes
     int col_batch_ = 2, row_batch_ = 2;         // autotuned per size
+    uint32_t tc_precision_ = LENIA_FFT_FP32;    // column DFT stages on the tensor cores
+    int tc_batch_ = 2;
     FastTables fast_{};
     float2* d_fast_tw_[4] = {nullptr, nullptr, nullptr, nullptr};
 

@@ -1,0 +1,85 @@
+"""Column DFT stages on the tensor cores (fftPrecision "bf16x3" / "fp16x3",
+split-precision operands with FP32 accumulation): per-step error against the
+FP64 oracle beside the FP32 CUDA-core path, at 512x256 and at 4096x4096
+(BASELINE config 4's size), plus the size fallback."""
+import numpy as np
+import pytest
+
+import life_simulation_b200 as lb
+from life_simulation_b200 import workloads as wl
+from oracle import lenia_oracle as lo
+from oracle.lenia_oracle import OracleLenia
+
+pytestmark = pytest.mark.gpu
+
+# Per-step max |GPU - FP64| bounds. FP32 is the spectral path's own bar; the
+# split-precision bounds follow from ~16 (BF16) and ~22 (FP16) significant
+# bits per DFT product, through the steep growth bells (sigma 0.0118).
+# Measured (B200): 512x256 max 4.6e-7 / 2.9e-6 / 1.2e-5, 4096^2 8.4e-7 /
+# 8.1e-6 / 2.5e-5 for fp32 / fp16x3 / bf16x3.
+TOL = {"fp32": 1e-5, "fp16x3": 2e-5, "bf16x3": 1e-4}
+PREC = {"fp32": lb.FFT_FP32, "bf16x3": lb.FFT_BF16X3, "fp16x3": lb.FFT_FP16X3}
+
+
+def step_errors(params, w, h, init, steps):
+    """Per-step (max, RMS) of |GPU - FP64|, both stepping from the GPU's
+    current state every step."""
+    m = lb.LeniaModule(params, w, h)
+    o = OracleLenia(params, w, h, "f64")
+    m.reset(3)
+    o.reset(3)
+    m.upload(init)
+    o.set_initial_field(init)
+    o.encode(0)  # builds the oracle's kernels; its state is replaced below
+    out, a = [], np.asarray(init, np.float32)
+    fp = m.frame_params(0)
+    for s in range(steps):
+        fp.frame_index = fp.audio_frame = s
+        m.upload(a)
+        m.step(fp, 1)
+        g = m.field()
+        o.state = a.astype(np.float64)
+        o.step_once(o.frame_params(), lo.pcg_hash(o.seed_ ^ (s * 197)), s, s)
+        d = g - o.state
+        out.append((float(np.abs(d).max()), float(np.sqrt(np.mean(d * d)))))
+        a = g
+    m.close()
+    return np.array(out)
+
+
+def tc_params(w, h, prec, radius=24):
+    p = wl.fft3_params(w, h)
+    p["fftPrecision"] = prec
+    p["radius"] = radius
+    return p
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp16x3", "bf16x3"])
+def test_tensor_core_columns_per_step_vs_fp64(prec):
+    w, h = 512, 256
+    params = tc_params(w, h, prec)
+    m = lb.LeniaModule(params, w, h)
+    assert m.warning == "" and m.info()["fft_precision"] == PREC[prec]
+    m.close()
+    init = wl.patches(w, h, 8, 64, seed=2)
+    errs = step_errors(params, w, h, init, 8)
+    assert errs[:, 0].max() <= TOL[prec], (prec, errs)
+
+
+def test_tensor_core_columns_4096():
+    """BASELINE config 4's field: 4096x4096, 3 kernels R=32."""
+    w = h = 4096
+    init = wl.patches(w, h, 40, 256, seed=2)
+    for prec in ("fp32", "fp16x3", "bf16x3"):
+        errs = step_errors(tc_params(w, h, prec, radius=32), w, h, init, 2)
+        assert errs[:, 0].max() <= TOL[prec], (prec, errs)
+        print(f"4096x4096 {prec}: per-step max {errs[:, 0].max():.2e} RMS {errs[:, 1].max():.2e}")
+
+
+def test_tensor_core_size_fallback():
+    m = lb.LeniaModule(tc_params(512, 512, "bf16x3"), 512, 512)
+    assert "fftPrecision" in m.warning and m.info()["fft_precision"] == lb.FFT_FP32
+    m.close()
+    m = lb.LeniaModule(tc_params(512, 256, "fp64"), 512, 256)
+    assert "fftPrecision" in m.warning and m.info()["fft_precision"] == lb.FFT_FP32
+    m.close()
