@@ -278,7 +278,8 @@ const char* lenia_batch_last_message(lenia_batch* b);
  * which every GPU that loads this library holds until the process exits.
  * No call allocates or frees device memory.
  *
- * field_in, field_out: distinct device buffers of height x width floats.
+ * field_in, field_out: distinct, 16-byte aligned device buffers of height x
+ *   width floats.
  * cfg: kernels, num_kernels (0: one kernel from fp's growth mu/sigma),
  *   radius, kernel_shell_sigma, kernel_core; its other fields are unused.
  * fp: the per-frame values; seed: the substep seed (the module uses

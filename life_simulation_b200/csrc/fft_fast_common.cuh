@@ -124,7 +124,8 @@ struct RowK {
     static constexpr int TABLES = (M + 1) + PI::tw_size() + PF::tw_size();
     static constexpr int BUF0 = (TABLES + 1) / 2 * 2;
     static_assert(PITCH % 2 == 0, "row pitch must keep 16-byte alignment");
-    static constexpr size_t smem() { return sizeof(float2) * (size_t(BUF0) + 2 * size_t(RB) * PITCH); }
+    // Tables plus `nbuf` buffers of RB rows.
+    static constexpr size_t smem(int nbuf = 2) { return sizeof(float2) * (size_t(BUF0) + nbuf * size_t(RB) * PITCH); }
 };
 
 // Real rows of W = 2M values are transformed as M complex values
@@ -144,6 +145,21 @@ __device__ __forceinline__ void stage_rows(float2* dst, const float2* __restrict
         if (b < rows) cp_async16(dst + b * PITCH + kb * KB + 2 * c2, plane + (size_t(kb) * H + y0 + b) * KB + 2 * c2);
     }
 }
+
+// Stages rows y0..y0+rows-1 of a row-major real field (W = 2M floats per
+// row) into shared rows of pitch PITCH, as M float2 pairs (x[2n], x[2n+1]):
+// 16-byte asynchronous copies. The caller waits.
+template <int M, int RB, int T, int PITCH>
+__device__ __forceinline__ void stage_field_rows(float2* dst, const float* __restrict__ field, int y0, int rows) {
+    for (int q = threadIdx.x; q < RB * (M / 2); q += T) {
+        const int c = q % (M / 2), b = q / (M / 2);
+        if (b < rows) cp_async16(dst + b * PITCH + 2 * c, field + (size_t(y0 + b) * M + 2 * c) * 2);
+    }
+}
+
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+// Waits until at most one committed group of this thread is still in flight.
+__device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
 // Inverse of the real-FFT split for element i of a staged half-spectrum row:
 // Z'[k] = (X[k] + conj X[M-k]) + i exp(+2 pi i k/W) (X[k] - conj X[M-k]);

@@ -107,7 +107,7 @@ __device__ __forceinline__ void block_add(double* red, float v) {
 // ------------------------------------------------------------------- rows
 
 template <class PI, int RB>
-__global__ void __launch_bounds__(RowK<PI, RB>::T)
+__global__ void __launch_bounds__(RowK<PI, RB>::T, (512 / RowK<PI, RB>::T > 1 ? 512 / RowK<PI, RB>::T : 1))
     row_adj_kernel(const AdjRowWorld* __restrict__ worlds, AdjRowArgs a, const float2* __restrict__ twr_g,
                    const float2* __restrict__ twi_g, const float2* __restrict__ twf_g) {
     using K = RowK<PI, RB>;
@@ -839,7 +839,7 @@ cudaError_t autotune(lenia_adjoint* a) {
         }
     }
     best = 1e30f;
-    for (int rb : {4, 2, 1}) {
+    for (int rb : lenia::kRowCandidates) {
         if (e != cudaSuccess) break;
         float ms = 0.0f;
         const cudaError_t r = timed([&] {

@@ -509,6 +509,46 @@ int lenia_batch_create(const lenia_world* worlds, uint32_t n, uint32_t policy, l
     }
     b.classes = kept;
 
+    // Columns / rows per CTA iteration of each size's passes: every candidate
+    // timed on the class's own tables (the fields are cleared afterwards).
+    if (!b.classes.empty()) {
+        cudaEvent_t ea, eb;
+        cudaEventCreate(&ea);
+        cudaEventCreate(&eb);
+        auto time_ms = [&](auto&& fn) {
+            float best = 1e30f;
+            for (int rep = 0; rep < 3; ++rep) {
+                cudaEventRecord(ea, b.stream);
+                if (fn() != cudaSuccess) return 1e30f;
+                cudaEventRecord(eb, b.stream);
+                cudaEventSynchronize(eb);
+                float ms = 0.0f;
+                cudaEventElapsedTime(&ms, ea, eb);
+                if (rep > 0) best = std::min(best, ms);
+            }
+            return best;
+        };
+        for (auto& c : b.classes) {
+            const int cnt = int(c.ids.size());
+            float best = 1e30f;
+            for (int cb : {8, 4, 2}) {
+                const float ms = time_ms([&] { return launch_col_fast_worlds(c.H, c.M, c.t, cb, c.d_stab[0], cnt, b.stream); });
+                if (ms < 0.97f * best) { best = ms; c.col_batch = cb; }
+            }
+            best = 1e30f;
+            for (int rb : kRowCandidates) {
+                const float ms = time_ms([&] {
+                    return launch_row_fast_worlds(c.H, c.M, c.t, c.tw_r2c, rb, c.d_stab[0], cnt, b.stream);
+                });
+                if (ms < 0.97f * best) { best = ms; c.row_batch = rb; }
+            }
+        }
+        cudaGetLastError();
+        cudaEventDestroy(ea);
+        cudaEventDestroy(eb);
+        cudaMemsetAsync(b.fields, 0, total * sizeof(float), b.stream);
+    }
+
     // Per-world seed/frame state and where each world's parameters live in
     // the two parity tables (device addresses, for the advance kernel).
     std::vector<StepParams*> loc(2 * size_t(n), nullptr);

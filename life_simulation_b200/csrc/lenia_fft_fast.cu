@@ -146,8 +146,17 @@ __global__ void __launch_bounds__(ColK<PF, B>::T)
 // nk > 0: inverse row transforms of U_k, growth, A' (+ the next step's row
 // spectrum when S_next != null). nk == 0: only the forward row transform of
 // A into S_next (the first step after an upload or init).
-template <class PI, int RB>
-__global__ void __launch_bounds__(RowK<PI, RB>::T)
+//
+// PIPE: software pipeline over two staging buffers and one work buffer.
+// While the rows of U_k go through their inverse transform, the rows of
+// U_{k+1} (after the last kernel: the rows of A) are already in flight by
+// cp.async, and while A' goes through the forward transform, the next row
+// group's U_0 is: a CTA always has one staged load in flight. Without PIPE
+// (one staging buffer, which doubles as the second work buffer) each item is
+// staged and waited for in turn: less shared memory per CTA, which wins
+// where shared memory limits the resident CTAs (long rows).
+template <class PI, int RB, bool PIPE>
+__global__ void __launch_bounds__(RowK<PI, RB>::T, (512 / RowK<PI, RB>::T > 1 ? 512 / RowK<PI, RB>::T : 1))
     row_fast_kernel(SpectralWorld w0, const SpectralWorld* __restrict__ worlds,
                     const float2* __restrict__ twr_g, const float2* __restrict__ twi_g,
                     const float2* __restrict__ twf_g) {
@@ -161,8 +170,9 @@ __global__ void __launch_bounds__(RowK<PI, RB>::T)
     float2* twr = sm;
     float2* twi = twr + (M + 1);
     float2* twf = twi + PI::tw_size();
-    float2* ba = sm + K::BUF0;  // stage (16-byte aligned), then ping-pong with bb
-    float2* bb = ba + RB * PITCH;
+    // Staging (16-byte aligned) and work buffers.
+    float2* stg[2] = {sm + K::BUF0, sm + K::BUF0 + (PIPE ? RB * PITCH : 0)};
+    float2* bw = sm + K::BUF0 + (PIPE ? 2 : 1) * RB * PITCH;
     copy_table(twr, twr_g, M + 1);
     copy_table(twi, twi_g, PI::tw_size());
     copy_table(twf, twf_g, PF::tw_size());
@@ -175,6 +185,20 @@ __global__ void __launch_bounds__(RowK<PI, RB>::T)
     const StepParams& p = sw.p;
     const bool asym = p.growth_mode == 1u;
     const bool jitter = p.mu_jitter > 0.0f;
+    // Item idx of a row group: the rows of U_idx for idx < nk, else of A.
+    const auto stage = [&](float2* dst, int y, int idx) {
+        if (y >= H) return;
+        const int n = min(RB, H - y);
+        if (idx < nk)
+            stage_rows<M, RB, T, PITCH>(dst, U + size_t(idx) * M * H, H, y, n);
+        else
+            stage_field_rows<M, RB, T, PITCH>(dst, A, y, n);
+    };
+    int base = 0;  // staging buffer of the group's first item
+    if constexpr (PIPE) {
+        stage(stg[0], int(blockIdx.x) * RB, 0);
+        cp_async_commit();
+    }
     for (int y0 = blockIdx.x * RB; y0 < H; y0 += gridDim.x * RB) {
         const int rows = min(RB, H - y0);
         int jj[K::ITL], bi[K::ITL];
@@ -188,16 +212,21 @@ __global__ void __launch_bounds__(RowK<PI, RB>::T)
         }
         float acc[K::ITL][RC][2];
         for (int kk = 0; kk < nk; ++kk) {
-            // Stage rows y0..y0+rows of U_k: per block, rows x 8 columns are
-            // contiguous (16-byte async copies, two columns each).
-            stage_rows<M, RB, T, PITCH>(ba, U + size_t(kk) * M * H, H, y0, rows);
-            cp_async_wait_all();
+            float2* cur = stg[(base + kk) & 1];
+            if constexpr (PIPE) {
+                stage(stg[(base + kk + 1) & 1], y0, kk + 1);
+                cp_async_commit();
+                cp_async_wait_prev();
+            } else {
+                stage(cur, y0, kk);
+                cp_async_wait_all();
+            }
             __syncthreads();
             // Inverse of the real-FFT split folded into the first pass's loads.
-            pass_gen<PI, 0, true, RB, T>([&](int b, int i) { return c2r_split<M>(ba + b * PITCH, twr, i); },
-                                         [&](int b, int i, float2 v) { bb[b * PITCH + i] = v; }, twi, rows);
+            pass_gen<PI, 0, true, RB, T>([&](int b, int i) { return c2r_split<M>(cur + b * PITCH, twr, i); },
+                                         [&](int b, int i, float2 v) { bw[b * PITCH + i] = v; }, twi, rows);
             __syncthreads();
-            float2* X = mid_passes<PI, 1, PI::np - 1, true, RB, T, PITCH>(bb, ba, twi, rows);
+            float2* X = mid_passes<PI, 1, PI::np - 1, true, RB, T, PITCH>(bw, cur, twi, rows);
             // Selects instead of a dynamic index into the parameter block (which
             // would spill it to local memory).
             const auto pick = [&](const float(&a)[kMaxKernels]) {
@@ -229,6 +258,18 @@ __global__ void __launch_bounds__(RowK<PI, RB>::T)
             }
             __syncthreads();
         }
+        // The rows of A are in sA; the other staging buffer takes the next
+        // row group's first item.
+        float2* sA = stg[(base + nk) & 1];
+        if constexpr (PIPE) {
+            stage(stg[(base + nk + 1) & 1], y0 + int(gridDim.x) * RB, 0);
+            cp_async_commit();
+            cp_async_wait_prev();
+        } else {
+            stage(sA, y0, nk);
+            cp_async_wait_all();
+        }
+        __syncthreads();
         // Euler step, noise, injection, clip (or, with nk == 0, the field as
         // is); the result is kept for the forward row transform (first
         // pass radix RC, the same elements per thread).
@@ -240,8 +281,7 @@ __global__ void __launch_bounds__(RowK<PI, RB>::T)
 #pragma unroll
             for (int t = 0; t < RC; ++t) {
                 const int n = jj[it] + t * NRC;
-                const size_t gi = size_t(gy) * W + 2 * n;
-                const float2 a = __ldg(reinterpret_cast<const float2*>(A + gi));
+                const float2 a = sA[bi[it] * PITCH + n];
                 if (nk == 0) {
                     za[it][t] = a;
                     continue;
@@ -251,27 +291,32 @@ __global__ void __launch_bounds__(RowK<PI, RB>::T)
                 g1.weighted = g1.std_sum = acc[it][t][1];
                 const float2 r = make_float2(growth_finish(p, a.x, g0, uint32_t(2 * n), uint32_t(gy)),
                                              growth_finish(p, a.y, g1, uint32_t(2 * n + 1), uint32_t(gy)));
-                *reinterpret_cast<float2*>(A_out + gi) = r;
+                *reinterpret_cast<float2*>(A_out + size_t(gy) * W + 2 * n) = r;
                 za[it][t] = r;
             }
         }
-        if (S_next == nullptr) continue;
+        if constexpr (PIPE) base = (base + nk + 1) & 1;
+        if (S_next == nullptr) {
+            __syncthreads();  // sA read before it is staged into again
+            continue;
+        }
 #pragma unroll
         for (int it = 0; it < K::ITL; ++it) {
             if (!ok[it]) continue;
             Dft<RC, false>::run(za[it]);
 #pragma unroll
-            for (int t = 0; t < RC; ++t) ba[bi[it] * PITCH + jj[it] * RC + t] = za[it][t];
+            for (int t = 0; t < RC; ++t) bw[bi[it] * PITCH + jj[it] * RC + t] = za[it][t];
         }
         __syncthreads();
-        float2* Y = mid_passes<PF, 1, PF::np - 1, false, RB, T, PITCH>(ba, bb, twf, rows);
-        float2* Zo = (Y == ba) ? bb : ba;
+        float2* Y = mid_passes<PF, 1, PF::np - 1, false, RB, T, PITCH>(bw, sA, twf, rows);
+        float2* Zo = (Y == bw) ? sA : bw;
         pass_gen<PF, PF::np - 1, false, RB, T>([&](int b, int i) { return Y[b * PITCH + i]; },
                                                 [&](int b, int i, float2 v) { Zo[b * PITCH + i] = v; }, twf, rows);
         __syncthreads();
         r2c_store_rows<M, RB, T, PITCH>(Zo, twr, S_next, H, y0, rows);
         __syncthreads();
     }
+    cp_async_wait_all();
 }
 
 // ------------------------------------------------------------- catalog
@@ -298,12 +343,12 @@ cudaError_t launch_col_t(const SpectralWorld& w0, const SpectralWorld* worlds, i
     return cudaGetLastError();
 }
 
-template <class PI, int RB>
+template <class PI, int RB, bool PIPE>
 cudaError_t launch_row_t(const SpectralWorld& w0, const SpectralWorld* worlds, int n, int H,
                          const float2* tw_r2c, const FastTables& t, cudaStream_t s) {
     using K = RowK<PI, RB>;
-    auto fn = row_fast_kernel<PI, RB>;
-    const size_t smem = K::smem();
+    auto fn = row_fast_kernel<PI, RB, PIPE>;
+    const size_t smem = K::smem(PIPE ? 3 : 2);
     if (smem > 227 * 1024) return cudaErrorInvalidConfiguration;
     cudaError_t e = prepare(fn, smem);
     if (e != cudaSuccess) return e;
@@ -383,12 +428,19 @@ cudaError_t col_dispatch(int H, int M, int batch, const SpectralWorld& w0, const
 
 cudaError_t row_dispatch(int H, int M, int batch, const SpectralWorld& w0, const SpectralWorld* worlds, int n,
                          const float2* tw_r2c, const FastTables& t, cudaStream_t s) {
+    const int rb = batch & ~kRowPipelined;
+    const bool pipe = (batch & kRowPipelined) != 0;
     switch (M) {
 #define X(m, ...)                                                                                  \
     case m:                                                                                        \
-        if (batch == 4) return launch_row_t<__VA_ARGS__, 4>(w0, worlds, n, H, tw_r2c, t, s);       \
-        if (batch == 2) return launch_row_t<__VA_ARGS__, 2>(w0, worlds, n, H, tw_r2c, t, s);       \
-        return launch_row_t<__VA_ARGS__, 1>(w0, worlds, n, H, tw_r2c, t, s);
+        if (pipe) {                                                                                \
+            if (rb == 4) return launch_row_t<__VA_ARGS__, 4, true>(w0, worlds, n, H, tw_r2c, t, s); \
+            if (rb == 2) return launch_row_t<__VA_ARGS__, 2, true>(w0, worlds, n, H, tw_r2c, t, s); \
+            return launch_row_t<__VA_ARGS__, 1, true>(w0, worlds, n, H, tw_r2c, t, s);              \
+        }                                                                                          \
+        if (rb == 4) return launch_row_t<__VA_ARGS__, 4, false>(w0, worlds, n, H, tw_r2c, t, s);    \
+        if (rb == 2) return launch_row_t<__VA_ARGS__, 2, false>(w0, worlds, n, H, tw_r2c, t, s);    \
+        return launch_row_t<__VA_ARGS__, 1, false>(w0, worlds, n, H, tw_r2c, t, s);
         LENIA_ROW_PLANS(X)
 #undef X
     default: return cudaErrorNotSupported;

@@ -118,8 +118,14 @@ void fast_plan_twiddles(const FastPlan& plan, std::vector<float2>& out);
 // M has no compile-time plan.
 bool fast_twiddle_tables(int H, int M, std::vector<float2> (&out)[4]);
 // batch: columns per CTA iteration (2, 4 or 8) / rows per CTA iteration
-// (1, 2 or 4). launch_row_fast with nk = 0 computes only the row spectrum of
-// A into S_next (U, A_out unused).
+// (1, 2 or 4), for the row pass optionally | kRowPipelined (the variant that
+// prefetches the next staged item while transforming the current one; it
+// needs a third shared buffer). launch_row_fast with nk = 0 computes only the
+// row spectrum of A into S_next (U, A_out unused). The row pass stages A with
+// 16-byte copies: A must be 16-byte aligned.
+constexpr int kRowPipelined = 0x100;
+// The row-batch candidates an autotuner times.
+constexpr int kRowCandidates[6] = {4, 2, 1, 4 | kRowPipelined, 2 | kRowPipelined, 1 | kRowPipelined};
 cudaError_t launch_col_fast(const FftGeometry& g, const FastTables& t, int batch, const float2* S,
                             float2* U, cudaStream_t s);
 cudaError_t launch_row_fast(const FftGeometry& g, const FastTables& t, int batch, const float2* U,

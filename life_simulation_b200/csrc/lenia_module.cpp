@@ -864,7 +864,7 @@ int LeniaModule::autotuneSpectral() {
         const float t = time_it([&] { return launch_col_fast(fgeo_, fast_, c, d_S_, d_U_, stream_); });
         if (t < 0.97f * best_col) { best_col = t; col_batch_ = c; }
     }
-    for (int c : {4, 2, 1}) {
+    for (int c : kRowCandidates) {
         const float t = time_it([&] {
             return launch_row_fast(fgeo_, fast_, c, d_U_, field_[0], field_[1], d_S_, p, fgeo_.nk, stream_);
         });

@@ -67,6 +67,9 @@ extern "C" int lenia_fft_step_noalloc(const float* field_in, float* field_out, u
     if (!field_in || !field_out || !cfg || !fp)
         return fail(LENIA_ERR_INVALID_ARG, "null argument");
     if (field_in == field_out) return fail(LENIA_ERR_INVALID_ARG, "field_in and field_out must differ");
+    // The row pass stages the field with 16-byte asynchronous copies.
+    if ((reinterpret_cast<uintptr_t>(field_in) | reinterpret_cast<uintptr_t>(field_out)) & 15u)
+        return fail(LENIA_ERR_INVALID_ARG, "field_in and field_out must be 16-byte aligned");
     if (!(fp->growth_sigma != 0.0f)) return fail(LENIA_ERR_INVALID_ARG, "growth_sigma must be nonzero");
     FftPlan prow{}, pcol{};
     if (width < 2 || (width & 1u) || height < 1 || !fft_plan(int(width / 2), prow) || !fft_plan(int(height), pcol))
