@@ -97,4 +97,31 @@ __device__ __forceinline__ float growth_finish(const StepParams& p, float A, con
     return fminf(fmaxf(A2, 0.0f), 1.0f);
 }
 
+// Out-of-line copies for kernels whose code size matters (the spectral row
+// pass): noise, injection and mu jitter are rare, and inlining them grows
+// the kernel past the instruction cache. Same arithmetic as above.
+static __device__ __noinline__ float growth_finish_call(const StepParams& p, float A, float weighted, float std_sum,
+                                                 uint32_t gx, uint32_t gy) {
+    GrowthAcc acc;
+    acc.weighted = weighted;
+    acc.std_sum = std_sum;
+    return growth_finish(p, A, acc, gx, gy);
+}
+static __device__ __noinline__ float mu_jitter_shift_call(const StepParams& p, uint32_t gx, uint32_t gy) {
+    return mu_jitter_shift(p, gx, gy);
+}
+// growth_finish with the common case (no noise, no injection) inline.
+__device__ __forceinline__ float growth_finish_lean(const StepParams& p, float A, float weighted, float std_sum,
+                                                    uint32_t gx, uint32_t gy) {
+    if (p.noise_amount > 0.0f || p.inject_amount > 0.0f) return growth_finish_call(p, A, weighted, std_sum, gx, gy);
+    float A2;
+    if (p.growth_mode == 1u) {
+        const float target = (p.sum_weights > 1e-6f) ? (weighted / p.sum_weights) : A;
+        A2 = A + p.dt * (target - A);
+    } else {
+        A2 = A + p.dt * std_sum;
+    }
+    return fminf(fmaxf(A2, 0.0f), 1.0f);
+}
+
 }  // namespace lenia

@@ -246,8 +246,8 @@ __global__ void __launch_bounds__(RowK<PI, RB>::T, (512 / RowK<PI, RB>::T > 1 ? 
 #pragma unroll
                 for (int t = 0; t < RC; ++t) {
                     const uint32_t x0 = uint32_t(2 * (jj[it] + t * NRC));
-                    const float m0 = jitter ? mu + mu_jitter_shift(p, x0, gy) : mu;
-                    const float m1 = jitter ? mu + mu_jitter_shift(p, x0 + 1u, gy) : mu;
+                    const float m0 = jitter ? mu + mu_jitter_shift_call(p, x0, gy) : mu;
+                    const float m1 = jitter ? mu + mu_jitter_shift_call(p, x0 + 1u, gy) : mu;
                     const float b0 = bell_fast(z[t].x, m0, inv_sigma);
                     const float b1 = bell_fast(z[t].y, m1, inv_sigma);
                     const float c0 = asym ? hw * b0 : hw * (2.0f * b0 - 1.0f);
@@ -286,11 +286,10 @@ __global__ void __launch_bounds__(RowK<PI, RB>::T, (512 / RowK<PI, RB>::T > 1 ? 
                     za[it][t] = a;
                     continue;
                 }
-                GrowthAcc g0, g1;
-                g0.weighted = g0.std_sum = acc[it][t][0];
-                g1.weighted = g1.std_sum = acc[it][t][1];
-                const float2 r = make_float2(growth_finish(p, a.x, g0, uint32_t(2 * n), uint32_t(gy)),
-                                             growth_finish(p, a.y, g1, uint32_t(2 * n + 1), uint32_t(gy)));
+                const float2 r =
+                    make_float2(growth_finish_lean(p, a.x, acc[it][t][0], acc[it][t][0], uint32_t(2 * n), uint32_t(gy)),
+                                growth_finish_lean(p, a.y, acc[it][t][1], acc[it][t][1], uint32_t(2 * n + 1),
+                                                   uint32_t(gy)));
                 *reinterpret_cast<float2*>(A_out + size_t(gy) * W + 2 * n) = r;
                 za[it][t] = r;
             }
