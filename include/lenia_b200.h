@@ -356,6 +356,75 @@ int lenia_adjoint_backward(lenia_adjoint* a, const float* g_final, float* g_init
 int lenia_adjoint_stats(lenia_adjoint* a, uint64_t* device_bytes, uint64_t* launches);
 const char* lenia_adjoint_last_message(lenia_adjoint* a);
 
+/* ---- Parameter bus and scenes ----
+ * The reference's ParameterBus (LifeCore/Params/ParameterBus.{h,cpp}) and
+ * scene loader (LifeCore/Params/Scene.cpp): a table of "<module>.<param>"
+ * values that a context reads its per-frame parameters from. Final value:
+ * the override if set, else ((set ?: base) + sum of adds) * product of muls,
+ * where the set/add/mul terms come from the mappings evaluated by the last
+ * lenia_bus_update. A context has its own bus unless one is attached; a
+ * scene's modules share one (SceneRunner, LifeCore/Sim/SceneRunner.cpp). The
+ * bus is host-side only (no device work). */
+typedef struct lenia_bus lenia_bus;
+enum { LENIA_MAP_ADD = 0, LENIA_MAP_SET = 1, LENIA_MAP_MUL = 2 };
+/* One mapping (AudioMappingSpec, ParameterBus.h:44-99). source: an input
+ * name (see lenia_bus_set_feature) or a time source
+ * "time.<sin|tri|ramp|noise>:<period s>[@<phase 0..1>]". in_max > in_min
+ * normalises the source to 0..1 first; then v * scale + offset, smoothed
+ * with time constant `smoothing` s (0: none), contributed to `target` in
+ * `mode` (LENIA_MAP_*). */
+typedef struct lenia_mapping {
+    const char* source;
+    const char* target;
+    float in_min, in_max;
+    float scale, offset;
+    float smoothing;
+    uint32_t mode;
+} lenia_mapping;
+typedef struct lenia_scene_info {
+    uint32_t seed, width, height;   /* "seed", "resolution" (1234, 1920x1080) */
+    uint32_t num_modules, num_mappings;
+} lenia_scene_info;
+int lenia_bus_create(uint32_t seed, lenia_bus** out);
+int lenia_bus_destroy(lenia_bus* bus);
+/* Scene::parse + applyBaseParams (Scene.cpp:24-113): the scene's seed,
+ * every module's numeric/boolean params as "<name>.<key>" bases, and the
+ * mappings of "audioMappings", "musicMappings" and "automation". A malformed
+ * time source fails the load (LENIA_ERR_PARSE), as in the reference. */
+int lenia_bus_load_scene(lenia_bus* bus, const char* scene_json, lenia_scene_info* info);
+int lenia_bus_add_mapping(lenia_bus* bus, const lenia_mapping* mapping);
+int lenia_bus_set_base(lenia_bus* bus, const char* key, float value);
+int lenia_bus_set_override(lenia_bus* bus, const char* key, float value);
+int lenia_bus_clear_override(lenia_bus* bus, const char* key);
+/* This frame's input values, by the reference's source names: audio
+ * channels kick/snare/hihat/perc/beat (".raw", ".smoothed", ".peak",
+ * ".trigger", ".hold"; the bare name is ".smoothed"), rms, low, mid, high,
+ * centroid, flux, time; "lane.<name>"; "section.energy", "section.progress",
+ * "section.changed"; events as "event:<type>.active" (1 while it runs),
+ * ".started", ".ended", ".progress" and its own curves "event:<type>.<curve>"
+ * (which have no value while the event does not run). Unset names read 0.
+ * Values persist until changed or cleared. */
+int lenia_bus_set_feature(lenia_bus* bus, const char* name, float value);
+/* The current section's role and index ("section.is:<role>", "section.n:<k>"). */
+int lenia_bus_set_section(lenia_bus* bus, const char* role, int32_t index);
+int lenia_bus_clear_features(lenia_bus* bus);
+/* ParameterBus::update (ParameterBus.cpp:267-343): evaluates every mapping
+ * and advances the bus clock (the time sources' input) by dt seconds. */
+int lenia_bus_update(lenia_bus* bus, float dt);
+/* param(ctx, key, fallback) for a full key ("lenia0.growthMu"). */
+int lenia_bus_value(lenia_bus* bus, const char* key, float fallback, float* out);
+const char* lenia_bus_last_message(lenia_bus* bus);
+/* The Lenia module of a scene document: the module named `module_name` (NULL:
+ * the first of type "Lenia"), set up from its params at the scene's
+ * resolution, its instance name the module's name. With `bus` (loaded from
+ * the same scene by lenia_bus_load_scene) the context reads that bus, which
+ * must outlive it; with NULL it gets its own bus loaded from the scene. */
+int lenia_create_scene_module(const char* scene_json, const char* module_name, lenia_bus* bus,
+                              const char* base_dir, lenia_ctx** out);
+/* Reads per-frame parameters from `bus` from now on (NULL: the context's own
+ * bus again). The bus must outlive the attachment. */
+int lenia_attach_bus(lenia_ctx* ctx, lenia_bus* bus);
+
 /* Message of the last warning or error on this context ("" if none). */
 const char* lenia_last_message(lenia_ctx* ctx);
 const char* lenia_status_string(int status);

@@ -99,7 +99,25 @@ EXPORTS = (
     "lenia_adjoint_create", "lenia_adjoint_destroy", "lenia_adjoint_set_params",
     "lenia_adjoint_forward", "lenia_adjoint_backward", "lenia_adjoint_stats",
     "lenia_adjoint_last_message",
+    "lenia_bus_create", "lenia_bus_destroy", "lenia_bus_load_scene", "lenia_bus_add_mapping",
+    "lenia_bus_set_base", "lenia_bus_set_override", "lenia_bus_clear_override", "lenia_bus_set_feature",
+    "lenia_bus_set_section", "lenia_bus_clear_features", "lenia_bus_update", "lenia_bus_value",
+    "lenia_bus_last_message", "lenia_create_scene_module", "lenia_attach_bus",
 )
+
+MAP_ADD, MAP_SET, MAP_MUL = 0, 1, 2
+
+
+class Mapping(ctypes.Structure):
+    """lenia_mapping (one audio/music/automation mapping)."""
+    _fields_ = [("source", ctypes.c_char_p), ("target", ctypes.c_char_p), ("in_min", ctypes.c_float),
+                ("in_max", ctypes.c_float), ("scale", ctypes.c_float), ("offset", ctypes.c_float),
+                ("smoothing", ctypes.c_float), ("mode", ctypes.c_uint32)]
+
+
+class SceneInfo(ctypes.Structure):
+    _fields_ = [("seed", ctypes.c_uint32), ("width", ctypes.c_uint32), ("height", ctypes.c_uint32),
+                ("num_modules", ctypes.c_uint32), ("num_mappings", ctypes.c_uint32)]
 
 ADJOINT_PARAMS_PER_KERNEL = 11
 ADJOINT_NUM_PARAMS = 45
@@ -192,6 +210,22 @@ def load_library(path: str = LIB_PATH):
     L.lenia_adjoint_stats.argtypes = [P, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]
     L.lenia_adjoint_last_message.argtypes = [P]
     L.lenia_adjoint_last_message.restype = ctypes.c_char_p
+    L.lenia_bus_create.argtypes = [u32, pp]
+    L.lenia_bus_destroy.argtypes = [P]
+    L.lenia_bus_load_scene.argtypes = [P, ctypes.c_char_p, ctypes.POINTER(SceneInfo)]
+    L.lenia_bus_add_mapping.argtypes = [P, ctypes.POINTER(Mapping)]
+    L.lenia_bus_set_base.argtypes = [P, ctypes.c_char_p, ctypes.c_float]
+    L.lenia_bus_set_override.argtypes = [P, ctypes.c_char_p, ctypes.c_float]
+    L.lenia_bus_clear_override.argtypes = [P, ctypes.c_char_p]
+    L.lenia_bus_set_feature.argtypes = [P, ctypes.c_char_p, ctypes.c_float]
+    L.lenia_bus_set_section.argtypes = [P, ctypes.c_char_p, ctypes.c_int32]
+    L.lenia_bus_clear_features.argtypes = [P]
+    L.lenia_bus_update.argtypes = [P, ctypes.c_float]
+    L.lenia_bus_value.argtypes = [P, ctypes.c_char_p, ctypes.c_float, ctypes.POINTER(ctypes.c_float)]
+    L.lenia_bus_last_message.argtypes = [P]
+    L.lenia_bus_last_message.restype = ctypes.c_char_p
+    L.lenia_create_scene_module.argtypes = [ctypes.c_char_p, ctypes.c_char_p, P, ctypes.c_char_p, pp]
+    L.lenia_attach_bus.argtypes = [P, P]
     for name in EXPORTS:
         getattr(L, name)  # raises AttributeError if the build lacks a symbol
     _LIB = L
@@ -349,6 +383,11 @@ class LeniaModule:
     def download_device(self, ptr: int, stream: Optional[int] = None) -> None:
         self._check(self._L.lenia_download_device(self._h, ctypes.c_void_p(ptr), self.width * self.height,
                                                   ctypes.c_void_p(stream) if stream else None))
+
+    def attach_bus(self, bus) -> None:
+        """Read per-frame parameters from a shared ParamBus (None: own bus)."""
+        self._check(self._L.lenia_attach_bus(self._h, bus._h if bus else None))
+        self._bus = bus
 
     def field_device_ptr(self) -> int:
         p = ctypes.c_void_p()
@@ -605,3 +644,92 @@ def unpack_param_grads(g: Sequence[float], num_betas: Sequence[int]) -> dict:
             "weight": [g[k * per + 2] for k in range(K)],
             "betas": [[g[k * per + 3 + j] for j in range(num_betas[k])] for k in range(K)],
             "dt": g[ADJOINT_NUM_PARAMS - 1]}
+
+
+class ParamBus:
+    """The parameter bus (lenia_bus_*): bases, overrides, mappings from
+    per-frame inputs and time sources, evaluated by update(dt). Host-only."""
+
+    def __init__(self, seed: int = 0):
+        L = load_library()
+        self._L = L
+        self._h = ctypes.c_void_p()
+        rc = L.lenia_bus_create(seed, ctypes.byref(self._h))
+        if rc < 0:
+            raise LeniaError(rc, "bus creation failed")
+
+    def _check(self, rc: int) -> int:
+        if rc < 0:
+            raise LeniaError(rc, self._L.lenia_bus_last_message(self._h).decode(errors="replace"))
+        return rc
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            self._L.lenia_bus_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def load_scene(self, scene) -> dict:
+        text = scene if isinstance(scene, str) else json.dumps(scene)
+        info = SceneInfo()
+        self._check(self._L.lenia_bus_load_scene(self._h, text.encode(), ctypes.byref(info)))
+        return {"seed": info.seed, "width": info.width, "height": info.height,
+                "num_modules": info.num_modules, "num_mappings": info.num_mappings}
+
+    def add_mapping(self, source: str, target: str, in_min=0.0, in_max=0.0, scale=1.0, offset=0.0,
+                    smoothing=0.0, mode: str = "add") -> None:
+        m = Mapping(source.encode(), target.encode(), in_min, in_max, scale, offset, smoothing,
+                    {"add": MAP_ADD, "set": MAP_SET, "mul": MAP_MUL, "multiply": MAP_MUL}.get(mode, MAP_ADD))
+        self._check(self._L.lenia_bus_add_mapping(self._h, ctypes.byref(m)))
+
+    def set_base(self, key: str, v: float) -> None:
+        self._check(self._L.lenia_bus_set_base(self._h, key.encode(), v))
+
+    def set_override(self, key: str, v: float) -> None:
+        self._check(self._L.lenia_bus_set_override(self._h, key.encode(), v))
+
+    def clear_override(self, key: str) -> None:
+        self._check(self._L.lenia_bus_clear_override(self._h, key.encode()))
+
+    def set_feature(self, name: str, v: float) -> None:
+        self._check(self._L.lenia_bus_set_feature(self._h, name.encode(), v))
+
+    def set_section(self, role: str, index: int) -> None:
+        self._check(self._L.lenia_bus_set_section(self._h, role.encode(), index))
+
+    def clear_features(self) -> None:
+        self._check(self._L.lenia_bus_clear_features(self._h))
+
+    def update(self, dt: float) -> None:
+        self._check(self._L.lenia_bus_update(self._h, dt))
+
+    def value(self, key: str, fallback: float = 0.0) -> float:
+        out = ctypes.c_float()
+        self._check(self._L.lenia_bus_value(self._h, key.encode(), fallback, ctypes.byref(out)))
+        return out.value
+
+
+def scene_module(scene, module_name: Optional[str] = None, bus: Optional[ParamBus] = None,
+                 base_dir: Optional[str] = None) -> "LeniaModule":
+    """The Lenia module of a scene document (lenia_create_scene_module)."""
+    L = load_library()
+    text = scene if isinstance(scene, str) else json.dumps(scene)
+    m = LeniaModule.__new__(LeniaModule)
+    m._L = L
+    m._h = ctypes.c_void_p()
+    rc = L.lenia_create_scene_module(text.encode(), module_name.encode() if module_name else None,
+                                     bus._h if bus else None, base_dir.encode() if base_dir else None,
+                                     ctypes.byref(m._h))
+    if rc < 0:
+        raise LeniaError(rc, L.lenia_last_message(None).decode(errors="replace"))
+    m.warning = L.lenia_last_message(m._h).decode(errors="replace") if rc > 0 else ""
+    m._bus = bus
+    w, h = ctypes.c_uint32(), ctypes.c_uint32()
+    m._check(L.lenia_field_size(m._h, ctypes.byref(w), ctypes.byref(h)))
+    m.width, m.height = w.value, h.value
+    return m

@@ -12,7 +12,15 @@
 
 struct lenia_ctx {
     lenia::LeniaModule module;
-    lenia::ParameterTable params;
+    lenia::ParameterBus own_bus;               // used unless a shared bus is attached
+    lenia::ParameterBus* bus = &own_bus;
+    std::string message;
+    std::string key(const char* k) const { return module.instance() + "." + k; }
+};
+
+// A parameter bus shared by the modules of a scene (SceneRunner's bus).
+struct lenia_bus {
+    lenia::ParameterBus bus;
     std::string message;
 };
 
@@ -36,6 +44,17 @@ int guarded(lenia_ctx* c, F&& f) {
         return LENIA_ERR_CUDA;
     } catch (const std::exception& e) {
         if (c) c->message = e.what();
+        return LENIA_ERR_STATE;
+    }
+}
+
+template <typename F>
+int bus_guarded(lenia_bus* b, F&& f) {
+    if (!b) return LENIA_ERR_INVALID_ARG;
+    try {
+        return f();
+    } catch (const std::exception& e) {
+        b->message = e.what();
         return LENIA_ERR_STATE;
     }
 }
@@ -122,12 +141,12 @@ int lenia_create_json(const char* params_json, uint32_t scene_w, uint32_t scene_
             return rc;
         }
         auto* c = new lenia_ctx();
+        c->module.configure("lenia0", std::move(mc));
         // Scene::applyBaseParams (Scene.cpp:96-113).
         for (const auto& m : j.members()) {
-            if (m.second.is_number()) c->params.setBase(m.first, float(m.second.as_number()));
-            else if (m.second.is_bool()) c->params.setBase(m.first, m.second.as_bool() ? 1.0f : 0.0f);
+            if (m.second.is_number()) c->own_bus.setBase(c->key(m.first.c_str()), float(m.second.as_number()));
+            else if (m.second.is_bool()) c->own_bus.setBase(c->key(m.first.c_str()), m.second.as_bool() ? 1.0f : 0.0f);
         }
-        c->module.configure("lenia0", std::move(mc));
         return finish_create(c, scene_w, scene_h, out);
     });
 }
@@ -172,7 +191,7 @@ int lenia_reset(lenia_ctx* c, uint32_t seed) {
 int lenia_set_param(lenia_ctx* c, const char* key, float value) {
     if (!c || !key) return LENIA_ERR_INVALID_ARG;
     return guarded(c, [&] {
-        c->params.setBase(key, value);
+        c->bus->setBase(c->key(key), value);
         return int(LENIA_OK);
     });
 }
@@ -180,7 +199,7 @@ int lenia_set_param(lenia_ctx* c, const char* key, float value) {
 int lenia_set_override(lenia_ctx* c, const char* key, float value) {
     if (!c || !key) return LENIA_ERR_INVALID_ARG;
     return guarded(c, [&] {
-        c->params.setOverride(key, value);
+        c->bus->setOverride(c->key(key), value);
         return int(LENIA_OK);
     });
 }
@@ -188,7 +207,7 @@ int lenia_set_override(lenia_ctx* c, const char* key, float value) {
 int lenia_clear_override(lenia_ctx* c, const char* key) {
     if (!c || !key) return LENIA_ERR_INVALID_ARG;
     return guarded(c, [&] {
-        c->params.clearOverride(key);
+        c->bus->clearOverride(c->key(key));
         return int(LENIA_OK);
     });
 }
@@ -196,7 +215,7 @@ int lenia_clear_override(lenia_ctx* c, const char* key) {
 int lenia_resolve_frame_params(lenia_ctx* c, uint32_t frame_index, uint32_t audio_frame,
                                lenia_frame_params* out) {
     if (!c || !out) return LENIA_ERR_INVALID_ARG;
-    *out = c->module.resolveFrameParams(c->params, frame_index, audio_frame);
+    *out = c->module.resolveFrameParams(*c->bus, frame_index, audio_frame);
     return LENIA_OK;
 }
 
@@ -205,7 +224,7 @@ int lenia_encode(lenia_ctx* c, uint32_t frame_index, uint32_t substeps, uint32_t
     if (!c) return LENIA_ERR_INVALID_ARG;
     return guarded(c, [&] {
         c->module.updateCPU(audio_frame);
-        return set_msg(c, c->module.encode(frame_index, substeps, c->params,
+        return set_msg(c, c->module.encode(frame_index, substeps, *c->bus,
                                            static_cast<cudaStream_t>(stream)));
     });
 }
@@ -331,6 +350,186 @@ int lenia_profile(lenia_ctx* c, int enable) {
 int lenia_profile_read(lenia_ctx* c, lenia_profile_data* out) {
     if (!c || !out) return LENIA_ERR_INVALID_ARG;
     return guarded(c, [&] { return c->module.readProfile(out); });
+}
+
+// ---------------------------------------------------------------- the bus
+
+int lenia_bus_create(uint32_t seed, lenia_bus** out) {
+    if (!out) return LENIA_ERR_INVALID_ARG;
+    *out = nullptr;
+    auto* b = new (std::nothrow) lenia_bus();
+    if (!b) return LENIA_ERR_STATE;
+    b->bus.setSeed(seed);
+    *out = b;
+    return LENIA_OK;
+}
+
+int lenia_bus_destroy(lenia_bus* b) {
+    if (!b) return LENIA_ERR_INVALID_ARG;
+    delete b;
+    return LENIA_OK;
+}
+
+int lenia_bus_load_scene(lenia_bus* b, const char* scene_json, lenia_scene_info* info) {
+    if (!scene_json) return LENIA_ERR_INVALID_ARG;
+    return bus_guarded(b, [&] {
+        std::string err;
+        const lenia::Json j = lenia::Json::parse(scene_json, &err);
+        lenia::SceneDoc sc;
+        if (!err.empty() || !lenia::parse_scene(j, sc, err)) {
+            b->message = err;
+            return int(LENIA_ERR_PARSE);
+        }
+        if (!lenia::apply_scene(sc, b->bus, err)) {
+            b->message = err;
+            return int(LENIA_ERR_PARSE);
+        }
+        if (info) {
+            info->seed = sc.seed;
+            info->width = sc.width;
+            info->height = sc.height;
+            info->num_modules = uint32_t(sc.modules.size());
+            info->num_mappings = uint32_t(sc.mappings.size());
+        }
+        return int(LENIA_OK);
+    });
+}
+
+int lenia_bus_add_mapping(lenia_bus* b, const lenia_mapping* m) {
+    if (!m || !m->source || !m->target || !m->source[0] || !m->target[0] || m->mode > LENIA_MAP_MUL)
+        return LENIA_ERR_INVALID_ARG;
+    return bus_guarded(b, [&] {
+        lenia::MappingSpec spec;
+        spec.source = m->source;
+        spec.target = m->target;
+        spec.in_min = m->in_min;
+        spec.in_max = m->in_max;
+        spec.scale = m->scale;
+        spec.offset = m->offset;
+        spec.smoothing = m->smoothing;
+        spec.mode = lenia::MapMode(m->mode);
+        std::string err;
+        if (!b->bus.addMapping(spec, err)) {
+            b->message = err;
+            return int(LENIA_ERR_INVALID_ARG);
+        }
+        return int(LENIA_OK);
+    });
+}
+
+int lenia_bus_set_base(lenia_bus* b, const char* key, float value) {
+    if (!key) return LENIA_ERR_INVALID_ARG;
+    return bus_guarded(b, [&] {
+        b->bus.setBase(key, value);
+        return int(LENIA_OK);
+    });
+}
+
+int lenia_bus_set_override(lenia_bus* b, const char* key, float value) {
+    if (!key) return LENIA_ERR_INVALID_ARG;
+    return bus_guarded(b, [&] {
+        b->bus.setOverride(key, value);
+        return int(LENIA_OK);
+    });
+}
+
+int lenia_bus_clear_override(lenia_bus* b, const char* key) {
+    if (!key) return LENIA_ERR_INVALID_ARG;
+    return bus_guarded(b, [&] {
+        b->bus.clearOverride(key);
+        return int(LENIA_OK);
+    });
+}
+
+int lenia_bus_set_feature(lenia_bus* b, const char* name, float value) {
+    if (!name) return LENIA_ERR_INVALID_ARG;
+    return bus_guarded(b, [&] {
+        b->bus.setFeature(name, value);
+        return int(LENIA_OK);
+    });
+}
+
+int lenia_bus_set_section(lenia_bus* b, const char* role, int32_t index) {
+    return bus_guarded(b, [&] {
+        b->bus.setSection(role ? role : "", index);
+        return int(LENIA_OK);
+    });
+}
+
+int lenia_bus_clear_features(lenia_bus* b) {
+    return bus_guarded(b, [&] {
+        b->bus.clearFeatures();
+        return int(LENIA_OK);
+    });
+}
+
+int lenia_bus_update(lenia_bus* b, float dt) {
+    return bus_guarded(b, [&] {
+        b->bus.update(dt);
+        return int(LENIA_OK);
+    });
+}
+
+int lenia_bus_value(lenia_bus* b, const char* key, float fallback, float* out) {
+    if (!key || !out) return LENIA_ERR_INVALID_ARG;
+    return bus_guarded(b, [&] {
+        *out = b->bus.value(key, fallback);
+        return int(LENIA_OK);
+    });
+}
+
+const char* lenia_bus_last_message(lenia_bus* b) { return b ? b->message.c_str() : ""; }
+
+int lenia_create_scene_module(const char* scene_json, const char* module_name, lenia_bus* bus,
+                              const char* base_dir, lenia_ctx** out) {
+    if (!scene_json || !out) return LENIA_ERR_INVALID_ARG;
+    *out = nullptr;
+    return guarded(nullptr, [&] {
+        std::string err;
+        const lenia::Json j = lenia::Json::parse(scene_json, &err);
+        lenia::SceneDoc sc;
+        if (!err.empty() || !lenia::parse_scene(j, sc, err)) {
+            g_create_error = err;
+            return int(LENIA_ERR_PARSE);
+        }
+        const lenia::SceneModule* mod = nullptr;
+        for (const auto& m : sc.modules)
+            if (module_name ? m.name == module_name : m.type == "Lenia") {
+                mod = &m;
+                break;
+            }
+        if (!mod) {
+            g_create_error = module_name ? "scene has no module named \"" + std::string(module_name) + "\""
+                                         : std::string("scene has no module of type \"Lenia\"");
+            return int(LENIA_ERR_INVALID_ARG);
+        }
+        if (mod->type != "Lenia") {
+            g_create_error = "module \"" + mod->name + "\" has type \"" + mod->type + "\", not \"Lenia\"";
+            return int(LENIA_ERR_INVALID_ARG);
+        }
+        lenia::ModuleConfig mc;
+        int rc = lenia::config_from_json(mod->params, base_dir ? base_dir : "", mc, err);
+        if (rc < 0) {
+            g_create_error = err;
+            return rc;
+        }
+        auto* c = new lenia_ctx();
+        c->module.configure(mod->name, std::move(mc));
+        if (bus) {
+            c->bus = &bus->bus;
+        } else if (!lenia::apply_scene(sc, c->own_bus, err)) {
+            g_create_error = err;
+            delete c;
+            return int(LENIA_ERR_PARSE);
+        }
+        return finish_create(c, sc.width, sc.height, out);
+    });
+}
+
+int lenia_attach_bus(lenia_ctx* c, lenia_bus* b) {
+    if (!c) return LENIA_ERR_INVALID_ARG;
+    c->bus = b ? &b->bus : &c->own_bus;
+    return LENIA_OK;
 }
 
 const char* lenia_last_message(lenia_ctx* c) {

@@ -28,17 +28,6 @@ uint32_t derive_seed(uint32_t global_seed, uint32_t tag) {  // Random.h:42-44
 
 static bool is_pow2(uint32_t v) { return v != 0 && (v & (v - 1u)) == 0; }
 
-float ParameterTable::value(const std::string& key, float fallback) const {
-    if (auto it = override_.find(key); it != override_.end()) return it->second;
-    float v;
-    if (auto it = set_.find(key); it != set_.end()) v = it->second;
-    else if (auto it2 = base_.find(key); it2 != base_.end()) v = it2->second;
-    else v = fallback;
-    if (auto it = add_.find(key); it != add_.end()) v += it->second;
-    if (auto it = mul_.find(key); it != mul_.end()) v *= it->second;
-    return v;
-}
-
 // -------------------------------------------------- kernel construction
 
 static double exp_core(double r) {
@@ -946,23 +935,26 @@ void LeniaModule::reset(uint32_t seed) {
     needs_kernel_init_ = true;
 }
 
-lenia_frame_params LeniaModule::resolveFrameParams(const ParameterTable& pt, uint32_t frame_index,
+// param(ctx, key, fallback) reads "<instance>.<key>" from the bus
+// (SimulationModule.h:120-123, Lenia.cpp:456-464).
+lenia_frame_params LeniaModule::resolveFrameParams(const ParameterBus& bus, uint32_t frame_index,
                                                    uint32_t audio_frame) const {
+    const auto param = [&](const char* key, float fallback) { return bus.value(instance_ + "." + key, fallback); };
     lenia_frame_params fp{};
-    fp.dt = pt.value("dt", fallback_dt_);
-    fp.growth_mu = pt.value("growthMu", fallback_mu_);
-    fp.growth_sigma = pt.value("growthSigma", fallback_sigma_);
-    fp.noise_amount = pt.value("noiseAmount", 0.0f);
-    fp.mu_jitter = pt.value("muJitter", 0.0f);
-    fp.inject_amount = pt.value("injectAmount", 0.0f);
-    fp.inject_count = uint32_t(pt.value("injectCount", 3.0f) + 0.5f);
-    fp.growth_mode = uint32_t(pt.value("growthMode", 1.0f) + 0.5f);
+    fp.dt = param("dt", fallback_dt_);
+    fp.growth_mu = param("growthMu", fallback_mu_);
+    fp.growth_sigma = param("growthSigma", fallback_sigma_);
+    fp.noise_amount = param("noiseAmount", 0.0f);
+    fp.mu_jitter = param("muJitter", 0.0f);
+    fp.inject_amount = param("injectAmount", 0.0f);
+    fp.inject_count = uint32_t(param("injectCount", 3.0f) + 0.5f);
+    fp.growth_mode = uint32_t(param("growthMode", 1.0f) + 0.5f);
     fp.frame_index = frame_index;
     fp.audio_frame = audio_frame;
     return fp;
 }
 
-int LeniaModule::encode(uint32_t frame_index, uint32_t substeps, const ParameterTable& params,
+int LeniaModule::encode(uint32_t frame_index, uint32_t substeps, const ParameterBus& params,
                         cudaStream_t stream) {
     return step(resolveFrameParams(params, frame_index, audio_frame_), substeps, stream);
 }

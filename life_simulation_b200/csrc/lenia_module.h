@@ -15,34 +15,9 @@
 #include "json_lite.h"
 #include "lenia_kernels.h"
 #include "lenia_types.h"
+#include "param_bus.h"
 
 namespace lenia {
-
-// ParameterBus read contract used by param(ctx, key, fallback)
-// (LifeCore/Params/ParameterBus.cpp:345-355): the override wins, else
-// ((set ?: base) + sum of adds) * product of muls.
-class ParameterTable {
-public:
-    void setBase(const std::string& key, float v) { base_[key] = v; }
-    void setOverride(const std::string& key, float v) { override_[key] = v; }
-    void clearOverride(const std::string& key) { override_.erase(key); }
-    void setMapped(const std::string& key, float v) { set_[key] = v; }
-    void addMapped(const std::string& key, float v) { add_[key] += v; }
-    void mulMapped(const std::string& key, float v) {
-        auto it = mul_.find(key);
-        if (it == mul_.end()) mul_[key] = v;
-        else it->second *= v;
-    }
-    void clearMapped() {
-        set_.clear();
-        add_.clear();
-        mul_.clear();
-    }
-    float value(const std::string& key, float fallback) const;
-
-private:
-    std::map<std::string, float> base_, override_, set_, add_, mul_;
-};
 
 struct KernelDef {  // Lenia.h:99-105
     float radius_scale = 1.0f;
@@ -107,12 +82,12 @@ public:
     void updateCPU(uint32_t audio_frame) { audio_frame_ = audio_frame; }
     // LeniaModule::encode (Lenia.cpp:455-644) with per-frame values read
     // from `params` (param(ctx, key, fallback)).
-    int encode(uint32_t frame_index, uint32_t substeps, const ParameterTable& params,
+    int encode(uint32_t frame_index, uint32_t substeps, const ParameterBus& params,
                cudaStream_t stream);
     // encode with explicit per-frame values.
     int step(const lenia_frame_params& fp, uint32_t substeps, cudaStream_t stream);
     // Per-frame values as encode would read them (Lenia.cpp:456-464).
-    lenia_frame_params resolveFrameParams(const ParameterTable& params, uint32_t frame_index,
+    lenia_frame_params resolveFrameParams(const ParameterBus& params, uint32_t frame_index,
                                           uint32_t audio_frame) const;
 
     // outputField (Lenia.h:63): the current state buffer on the device.
@@ -126,6 +101,7 @@ public:
     uint32_t height() const { return h_; }
     void info(lenia_info* out) const;
     const std::string& message() const { return message_; }
+    const std::string& instance() const { return instance_; }
     void setMessage(std::string m) { message_ = std::move(m); }
     cudaStream_t stream() const { return stream_; }
 

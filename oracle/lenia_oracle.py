@@ -447,6 +447,94 @@ class OracleLenia:
 
 # ------------------------------------------------------- compiled reference
 
+class RefEventIn(ctypes.Structure):
+    _fields_ = [("type", ctypes.c_char * 32), ("curve", ctypes.c_char * 32), ("curve_value", ctypes.c_float),
+                ("progress", ctypes.c_float), ("started", ctypes.c_int32), ("ended", ctypes.c_int32)]
+
+
+class RefFeaturesIn(ctypes.Structure):
+    """Per-frame inputs of the reference's bus (ref_shim/ref_runtime.cpp)."""
+    _fields_ = [("env", (ctypes.c_float * 5) * 5), ("scalars", ctypes.c_float * 7), ("lanes", ctypes.c_float * 10),
+                ("section_index", ctypes.c_int32), ("section_energy", ctypes.c_float),
+                ("section_progress", ctypes.c_float), ("section_changed", ctypes.c_int32),
+                ("section_role", ctypes.c_char * 32), ("num_events", ctypes.c_int32), ("events", RefEventIn * 4)]
+
+
+REF_ENV_CHANNELS = ("kick", "snare", "hihat", "perc", "beat")
+REF_ENV_PARTS = ("raw", "smoothed", "peak", "trigger", "hold")
+REF_SCALARS = ("rms", "low", "mid", "high", "centroid", "flux", "time")
+REF_LANES = ("tension", "intensity", "wet_ratio", "kick_gate", "macro_density", "macro_intensity",
+             "master_rms", "drums_rms", "spatial_active", "se_env")
+
+
+class RefBus:
+    """The reference's ParameterBus (LifeCore/Params/ParameterBus.cpp), on its
+    own or the bus of a RefLenia session."""
+
+    def __init__(self, seed: int = 0, session: "Optional[RefLenia]" = None):
+        L = RefLenia.lib()
+        self._L = L
+        self._own = session is None
+        self.h_ = L.ref_bus_create(seed) if self._own else L.ref_session_bus(session.h_)
+        self._session = session
+
+    def __del__(self):
+        if getattr(self, "_own", False) and getattr(self, "h_", None):
+            self._L.ref_bus_destroy(self.h_)
+
+    def load_scene(self, scene) -> None:
+        err = ctypes.create_string_buffer(512)
+        text = scene if isinstance(scene, str) else json.dumps(scene)
+        if self._L.ref_bus_load_scene(self.h_, text.encode(), err, 512) != 0:
+            raise ValueError(err.value.decode())
+
+    def add_mapping(self, source, target, in_min=0.0, in_max=0.0, scale=1.0, offset=0.0, smoothing=0.0,
+                    mode="add") -> None:
+        if self._L.ref_bus_add_mapping(self.h_, source.encode(), target.encode(), in_min, in_max, scale, offset,
+                                       smoothing, mode.encode()) != 0:
+            raise ValueError(f"bad time source {source!r}")
+
+    def set_base(self, key, v):
+        self._L.ref_bus_set_base(self.h_, key.encode(), v)
+
+    def set_override(self, key, v):
+        self._L.ref_bus_set_override(self.h_, key.encode(), v)
+
+    def clear_override(self, key):
+        self._L.ref_bus_clear_override(self.h_, key.encode())
+
+    def update(self, features: dict, dt: float, section_role: str = "", section_index: int = -1,
+               events: Sequence[dict] = ()) -> None:
+        """features: the names lenia_bus_set_feature takes ("kick.raw",
+        "rms", "lane.tension", "section.energy", ...); events: dicts with
+        type, progress, started, ended and optionally curve/curve_value."""
+        f = RefFeaturesIn()
+        for c, ch in enumerate(REF_ENV_CHANNELS):
+            for p, part in enumerate(REF_ENV_PARTS):
+                f.env[c][p] = features.get(f"{ch}.{part}", 0.0)
+        for i, n in enumerate(REF_SCALARS):
+            f.scalars[i] = features.get(n, 0.0)
+        for i, n in enumerate(REF_LANES):
+            f.lanes[i] = features.get("lane." + n, 0.0)
+        f.section_index = section_index
+        f.section_energy = features.get("section.energy", 0.0)
+        f.section_progress = features.get("section.progress", 0.0)
+        f.section_changed = int(features.get("section.changed", 0.0) != 0.0)
+        f.section_role = section_role.encode()
+        f.num_events = len(events)
+        for i, e in enumerate(events):
+            f.events[i].type = e["type"].encode()
+            f.events[i].curve = e.get("curve", "").encode()
+            f.events[i].curve_value = e.get("curve_value", 0.0)
+            f.events[i].progress = e.get("progress", 0.0)
+            f.events[i].started = int(e.get("started", False))
+            f.events[i].ended = int(e.get("ended", False))
+        self._L.ref_bus_update(self.h_, ctypes.byref(f), dt)
+
+    def value(self, key, fallback=0.0) -> float:
+        return self._L.ref_bus_value(self.h_, key.encode(), fallback)
+
+
 class RefLenia:
     """The reference's own Lenia module + shaders compiled for the CPU."""
 
@@ -482,6 +570,21 @@ class RefLenia:
             L.ref_pcg.argtypes = [u32]
             L.ref_rand.restype = ctypes.c_float
             L.ref_rand.argtypes = [u32, u32, u32, u32]
+            L.ref_bus_create.restype = P
+            L.ref_bus_create.argtypes = [u32]
+            L.ref_bus_destroy.argtypes = [P]
+            L.ref_bus_load_scene.argtypes = [P, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_size_t]
+            L.ref_bus_add_mapping.argtypes = [P, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_float,
+                                              ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                              ctypes.c_char_p]
+            L.ref_bus_set_base.argtypes = [P, ctypes.c_char_p, ctypes.c_float]
+            L.ref_bus_set_override.argtypes = [P, ctypes.c_char_p, ctypes.c_float]
+            L.ref_bus_clear_override.argtypes = [P, ctypes.c_char_p]
+            L.ref_bus_update.argtypes = [P, ctypes.POINTER(RefFeaturesIn), ctypes.c_float]
+            L.ref_bus_value.restype = ctypes.c_float
+            L.ref_bus_value.argtypes = [P, ctypes.c_char_p, ctypes.c_float]
+            L.ref_session_bus.restype = P
+            L.ref_session_bus.argtypes = [P]
             cls._L = L
         return cls._L
 

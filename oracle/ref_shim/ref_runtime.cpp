@@ -20,6 +20,7 @@
 #include "LifeCore/Metal/CommandGraph.h"
 #include "LifeCore/Metal/ResourcePool.h"
 #include "LifeCore/Params/ParameterBus.h"
+#include "LifeCore/Params/Scene.h"
 #include "LifeCore/Render/ColorMapPass.h"
 #include "LifeCore/Sim/SimulationModule.h"
 #include "Modules/FieldModules/Lenia.h"
@@ -377,6 +378,126 @@ size_t ref_pass_label(void* h, uint64_t i, char* buf, size_t cap) {
 void ref_clear_pass_log(void* h) {
     auto* s = static_cast<RefSession*>(h);
     s->graph.impl().passLabels.clear();
+}
+
+// ---- The reference's parameter bus alone (LifeCore/Params/ParameterBus.cpp,
+// Scene.cpp), driven with synthetic per-frame inputs.
+struct RefEventIn {
+    char type[32];
+    char curve[32];
+    float curve_value;
+    float progress;
+    int32_t started, ended;
+};
+struct RefFeaturesIn {
+    float env[5][5];   // kick, snare, hihat, perc, beat x raw, smoothed, peak, trigger, hold
+    float scalars[7];  // rms, low, mid, high, centroid, flux, time
+    float lanes[10];   // tension, intensity, wetRatio, kickGate, macroDensity, macroIntensity,
+                       // masterRms, drumsRms, spatialActive, seEnv
+    int32_t section_index;
+    float section_energy, section_progress;
+    int32_t section_changed;
+    char section_role[32];
+    int32_t num_events;
+    RefEventIn events[4];
+};
+
+void* ref_bus_create(uint32_t seed) {
+    auto* b = new life::ParameterBus();
+    b->setSeed(seed);
+    return b;
+}
+void ref_bus_destroy(void* b) { delete static_cast<life::ParameterBus*>(b); }
+
+// Scene::parse + applyBaseParams; 0 or -1 with the message in err.
+int ref_bus_load_scene(void* b, const char* json_text, char* err, size_t err_n) {
+    std::string e;
+    try {
+        auto j = nlohmann::json::parse(json_text);
+        auto sc = life::Scene::parse(j, e);
+        if (!sc) {
+            std::snprintf(err, err_n, "%s", e.c_str());
+            return -1;
+        }
+        sc->applyBaseParams(*static_cast<life::ParameterBus*>(b));
+    } catch (const std::exception& ex) {
+        std::snprintf(err, err_n, "%s", ex.what());
+        return -1;
+    }
+    return 0;
+}
+
+// Scene::parse's time-source check, then addMapping; 0 or -1.
+int ref_bus_add_mapping(void* b, const char* source, const char* target, float in_min, float in_max,
+                        float scale, float offset, float smoothing, const char* mode) {
+    life::TimeSourceKind k;
+    float per, ph;
+    std::string e;
+    if (!life::parseTimeSource(source, k, per, ph, e)) return -1;
+    life::AudioMappingSpec m;
+    m.source = source;
+    m.target = target;
+    m.inMin = in_min;
+    m.inMax = in_max;
+    m.scale = scale;
+    m.offset = offset;
+    m.smoothing = smoothing;
+    m.mode = life::mappingModeFromString(mode);
+    static_cast<life::ParameterBus*>(b)->addMapping(m);
+    return 0;
+}
+
+void ref_bus_set_base(void* b, const char* key, float v) { static_cast<life::ParameterBus*>(b)->setBase(key, v); }
+void ref_bus_set_override(void* b, const char* key, float v) {
+    static_cast<life::ParameterBus*>(b)->setOverride(key, v);
+}
+void ref_bus_clear_override(void* b, const char* key) { static_cast<life::ParameterBus*>(b)->clearOverride(key); }
+
+void ref_bus_update(void* b, const RefFeaturesIn* f, float dt) {
+    life::MusicFeatureState m;
+    life::ChannelEnvelope* envs[5] = {&m.audio.kickEnv, &m.audio.snareEnv, &m.audio.hihatEnv, &m.audio.percEnv,
+                                      &m.audio.beatEnv};
+    for (int c = 0; c < 5; ++c) *envs[c] = {f->env[c][0], f->env[c][1], f->env[c][2], f->env[c][3], f->env[c][4]};
+    m.audio.rms = f->scalars[0];
+    m.audio.low = f->scalars[1];
+    m.audio.mid = f->scalars[2];
+    m.audio.high = f->scalars[3];
+    m.audio.centroid = f->scalars[4];
+    m.audio.flux = f->scalars[5];
+    m.audio.time = f->scalars[6];
+    float* lanes[10] = {&m.lanes.tension, &m.lanes.intensity, &m.lanes.wetRatio, &m.lanes.kickGate,
+                        &m.lanes.macroDensity, &m.lanes.macroIntensity, &m.lanes.masterRms, &m.lanes.drumsRms,
+                        &m.lanes.spatialActive, &m.lanes.seEnv};
+    for (int i = 0; i < 10; ++i) *lanes[i] = f->lanes[i];
+    m.sectionIndex = f->section_index;
+    m.sectionRole = f->section_role;
+    m.sectionEnergy = f->section_energy;
+    m.sectionProgress = f->section_progress;
+    m.sectionChanged = f->section_changed != 0;
+    std::vector<life::MusicEvent> defs(size_t(std::max(0, f->num_events)));
+    for (int i = 0; i < f->num_events; ++i) {
+        defs[i].type = f->events[i].type;
+        defs[i].frameStart = 0;
+        defs[i].frameEnd = 1;
+        if (f->events[i].curve[0]) defs[i].curves.push_back({f->events[i].curve, {f->events[i].curve_value}});
+    }
+    for (int i = 0; i < f->num_events; ++i) {
+        life::ActiveEvent a;
+        a.def = &defs[i];
+        a.progress = f->events[i].progress;
+        a.justStarted = f->events[i].started != 0;
+        a.justEnded = f->events[i].ended != 0;
+        m.events.push_back(a);
+    }
+    m.frame = 0;
+    static_cast<life::ParameterBus*>(b)->update(m, dt);
+}
+
+// The bus a Lenia session reads its parameters from (not to be destroyed).
+void* ref_session_bus(void* h) { return &static_cast<RefSession*>(h)->bus; }
+
+float ref_bus_value(void* b, const char* key, float fallback) {
+    return static_cast<life::ParameterBus*>(b)->value(key, fallback);
 }
 
 uint32_t ref_pcg(uint32_t v) { return ref_pcg_hash(v); }
