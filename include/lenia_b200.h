@@ -219,6 +219,7 @@ enum {
     LENIA_PHASE_ROW_FFT = 2,    /* row pass A -> row spectrum */
     LENIA_PHASE_COLUMN = 3,     /* column FFT, spectrum products, inverse */
     LENIA_PHASE_ROW_GROWTH = 4, /* inverse row pass + growth (+ next row FFT) */
+    LENIA_PHASE_COLORMAP = 5,   /* field -> RGBA16F colour layer */
     LENIA_PHASE_COUNT = 8
 };
 typedef struct lenia_profile_data {
@@ -355,6 +356,30 @@ int lenia_adjoint_backward(lenia_adjoint* a, const float* g_final, float* g_init
 /* Device memory held, and launches issued since creation. */
 int lenia_adjoint_stats(lenia_adjoint* a, uint64_t* device_bytes, uint64_t* launches);
 const char* lenia_adjoint_last_message(lenia_adjoint* a);
+
+/* ---- Colour map (the module's output layer) ----
+ * The field as an RGBA16F image through the module's cosine palette
+ * (Shaders/Render/ColorMap.metal: t = clamp(v * input_scale + input_bias,
+ * 0, 1), rgb = max(a + b cos(2 pi (c t + d)), 0) * exposure, alpha = t; v
+ * the channel `channel` of the field read as (A, 0, 0, 1)). The palette is
+ * the reference Lenia module's (ColorMapPass defaults with d = (0.60, 0.45,
+ * 0.30), channel 0, Lenia.cpp:349-354) updated by the params' "colorMap"
+ * block (ColorMapPass.cpp:70-101). */
+typedef struct lenia_colormap {
+    float a[3], b[3], c[3], d[3];
+    float input_scale, input_bias, exposure;
+    uint32_t channel;
+} lenia_colormap;
+int lenia_get_colormap(lenia_ctx* ctx, lenia_colormap* out);
+int lenia_set_colormap(lenia_ctx* ctx, const lenia_colormap* cm);
+/* The palette a params JSON object gives (host only, no device). */
+int lenia_colormap_from_json(const char* params_json, lenia_colormap* out);
+/* The current field's colour layer into `dst` (device, width x height
+ * pixels of 4 halves, RGBA): colorMapField when the size is the field's,
+ * else colorMapFieldScaled (bilinear, wrapping, at output pixel centres) --
+ * the module's output at the scene resolution (Lenia.cpp:646-652).
+ * Asynchronous on `stream` after the queued steps. */
+int lenia_render_rgba16f(lenia_ctx* ctx, void* dst, uint32_t width, uint32_t height, void* stream);
 
 /* ---- Parameter bus and scenes ----
  * The reference's ParameterBus (LifeCore/Params/ParameterBus.{h,cpp}) and

@@ -103,7 +103,20 @@ EXPORTS = (
     "lenia_bus_set_base", "lenia_bus_set_override", "lenia_bus_clear_override", "lenia_bus_set_feature",
     "lenia_bus_set_section", "lenia_bus_clear_features", "lenia_bus_update", "lenia_bus_value",
     "lenia_bus_last_message", "lenia_create_scene_module", "lenia_attach_bus",
+    "lenia_get_colormap", "lenia_set_colormap", "lenia_colormap_from_json", "lenia_render_rgba16f",
 )
+
+
+class ColorMap(ctypes.Structure):
+    """lenia_colormap (the module's cosine palette)."""
+    _fields_ = [("a", ctypes.c_float * 3), ("b", ctypes.c_float * 3), ("c", ctypes.c_float * 3),
+                ("d", ctypes.c_float * 3), ("input_scale", ctypes.c_float), ("input_bias", ctypes.c_float),
+                ("exposure", ctypes.c_float), ("channel", ctypes.c_uint32)]
+
+    def as_dict(self) -> dict:
+        return {"a": list(self.a), "b": list(self.b), "c": list(self.c), "d": list(self.d),
+                "inputScale": self.input_scale, "inputBias": self.input_bias, "exposure": self.exposure,
+                "channel": self.channel}
 
 MAP_ADD, MAP_SET, MAP_MUL = 0, 1, 2
 
@@ -140,7 +153,7 @@ class World(ctypes.Structure):
                 ("growth_mode", ctypes.c_uint32), ("kernel_core", ctypes.c_uint32),
                 ("shell_mu", ctypes.c_float), ("shell_sigma", ctypes.c_float), ("seed", ctypes.c_uint32)]
 
-PHASES = ("init", "direct", "row_fft", "column", "row_growth")
+PHASES = ("init", "direct", "row_fft", "column", "row_growth", "colormap")
 
 
 class ProfileData(ctypes.Structure):
@@ -226,6 +239,10 @@ def load_library(path: str = LIB_PATH):
     L.lenia_bus_last_message.restype = ctypes.c_char_p
     L.lenia_create_scene_module.argtypes = [ctypes.c_char_p, ctypes.c_char_p, P, ctypes.c_char_p, pp]
     L.lenia_attach_bus.argtypes = [P, P]
+    L.lenia_get_colormap.argtypes = [P, ctypes.POINTER(ColorMap)]
+    L.lenia_set_colormap.argtypes = [P, ctypes.POINTER(ColorMap)]
+    L.lenia_colormap_from_json.argtypes = [ctypes.c_char_p, ctypes.POINTER(ColorMap)]
+    L.lenia_render_rgba16f.argtypes = [P, P, u32, u32, P]
     for name in EXPORTS:
         getattr(L, name)  # raises AttributeError if the build lacks a symbol
     _LIB = L
@@ -383,6 +400,19 @@ class LeniaModule:
     def download_device(self, ptr: int, stream: Optional[int] = None) -> None:
         self._check(self._L.lenia_download_device(self._h, ctypes.c_void_p(ptr), self.width * self.height,
                                                   ctypes.c_void_p(stream) if stream else None))
+
+    def colormap(self) -> ColorMap:
+        cm = ColorMap()
+        self._check(self._L.lenia_get_colormap(self._h, ctypes.byref(cm)))
+        return cm
+
+    def set_colormap(self, cm: ColorMap) -> None:
+        self._check(self._L.lenia_set_colormap(self._h, ctypes.byref(cm)))
+
+    def render_device(self, ptr: int, width: int, height: int, stream: Optional[int] = None) -> None:
+        """Colour layer (RGBA16F, 8 bytes per pixel) into a device buffer."""
+        self._check(self._L.lenia_render_rgba16f(self._h, ctypes.c_void_p(ptr), width, height,
+                                                 ctypes.c_void_p(stream) if stream else None))
 
     def attach_bus(self, bus) -> None:
         """Read per-frame parameters from a shared ParamBus (None: own bus)."""
@@ -733,3 +763,14 @@ def scene_module(scene, module_name: Optional[str] = None, bus: Optional[ParamBu
     m._check(L.lenia_field_size(m._h, ctypes.byref(w), ctypes.byref(h)))
     m.width, m.height = w.value, h.value
     return m
+
+
+def colormap_from_params(params) -> ColorMap:
+    """The palette a module's params give (no device)."""
+    L = load_library()
+    text = params if isinstance(params, str) else json.dumps(params)
+    cm = ColorMap()
+    rc = L.lenia_colormap_from_json(text.encode(), ctypes.byref(cm))
+    if rc < 0:
+        raise LeniaError(rc, L.lenia_last_message(None).decode(errors="replace"))
+    return cm

@@ -352,6 +352,48 @@ int lenia_profile_read(lenia_ctx* c, lenia_profile_data* out) {
     return guarded(c, [&] { return c->module.readProfile(out); });
 }
 
+// ---------------------------------------------------------- colour map
+
+static_assert(sizeof(lenia_colormap) == sizeof(lenia::ColorMapParams), "colour map layout");
+
+int lenia_get_colormap(lenia_ctx* c, lenia_colormap* out) {
+    if (!c || !out) return LENIA_ERR_INVALID_ARG;
+    std::memcpy(out, &c->module.colormap(), sizeof(*out));
+    return LENIA_OK;
+}
+
+int lenia_set_colormap(lenia_ctx* c, const lenia_colormap* cm) {
+    if (!c || !cm) return LENIA_ERR_INVALID_ARG;
+    lenia::ColorMapParams p;
+    std::memcpy(&p, cm, sizeof(p));
+    c->module.setColormap(p);
+    return LENIA_OK;
+}
+
+int lenia_colormap_from_json(const char* params_json, lenia_colormap* out) {
+    if (!params_json || !out) return LENIA_ERR_INVALID_ARG;
+    return guarded(nullptr, [&] {
+        std::string err;
+        const lenia::Json j = lenia::Json::parse(params_json, &err);
+        if (!err.empty()) {
+            g_create_error = err;
+            return int(LENIA_ERR_PARSE);
+        }
+        lenia::ColorMapParams p = lenia::lenia_default_colormap();
+        lenia::colormap_from_json(j, p);
+        std::memcpy(out, &p, sizeof(*out));
+        return int(LENIA_OK);
+    });
+}
+
+int lenia_render_rgba16f(lenia_ctx* c, void* dst, uint32_t width, uint32_t height, void* stream) {
+    if (!c) return LENIA_ERR_INVALID_ARG;
+    return guarded(c, [&] {
+        cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c->module.stream();
+        return set_msg(c, c->module.render(dst, width, height, s));
+    });
+}
+
 // ---------------------------------------------------------------- the bus
 
 int lenia_bus_create(uint32_t seed, lenia_bus** out) {

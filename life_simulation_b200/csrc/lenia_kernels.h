@@ -147,6 +147,16 @@ bool tc_col_plan(int H);
 cudaError_t launch_col_tc(const FftGeometry& g, const FastTables& t, int precision, int batch, const float2* S,
                           float2* U, cudaStream_t s);
 
+// Colour map (lenia_colormap.cu): the field (w x h) to ow x oh RGBA16F
+// (ushort4 per pixel); bilinear with wrapping when the sizes differ.
+struct ColorMapParams {  // ColorMapParams, Shaders/Render/ColorMap.metal:6-15
+    float a[3], b[3], c[3], d[3];
+    float input_scale, input_bias, exposure;
+    uint32_t channel;
+};
+cudaError_t launch_colormap(const float* field, int w, int h, const ColorMapParams& p, void* rgba16f, int ow,
+                            int oh, cudaStream_t s);
+
 // ------------------------------------------------------------------ inits
 cudaError_t launch_init_noise(float* A, const InitParams& p, cudaStream_t s);
 cudaError_t launch_init_stamp(float* A, uint32_t w, uint32_t h, const float* org, uint32_t ow,

@@ -294,6 +294,44 @@ static bool load_organism_file(const std::string& path, OrganismData& out, std::
     return true;
 }
 
+ColorMapParams lenia_default_colormap() {
+    ColorMapParams cm{};
+    for (int i = 0; i < 3; ++i) {
+        cm.a[i] = 0.5f;
+        cm.b[i] = 0.5f;
+        cm.c[i] = 1.0f;
+    }
+    cm.d[0] = 0.60f;
+    cm.d[1] = 0.45f;
+    cm.d[2] = 0.30f;
+    cm.input_scale = 1.0f;
+    cm.input_bias = 0.0f;
+    cm.exposure = 1.0f;
+    cm.channel = 0;
+    return cm;
+}
+
+void colormap_from_json(const Json& params, ColorMapParams& cm) {
+    const Json* j = params.find("colorMap");
+    if (!j || !j->is_object()) return;
+    if (j->value_string("palette", "") == "mono") {  // black (t = 0) to white (t = 1)
+        for (int i = 0; i < 3; ++i) cm.a[i] = cm.b[i] = cm.c[i] = cm.d[i] = 0.5f;
+    }
+    const auto vec3 = [&](const char* key, float* v) {
+        const Json* a = j->find(key);
+        if (a && a->is_array() && a->size() >= 3)
+            for (int i = 0; i < 3; ++i) v[i] = float(a->items()[size_t(i)].as_number());
+    };
+    vec3("a", cm.a);
+    vec3("b", cm.b);
+    vec3("c", cm.c);
+    vec3("d", cm.d);
+    cm.input_scale = j->value_float("inputScale", cm.input_scale);
+    cm.input_bias = j->value_float("inputBias", cm.input_bias);
+    cm.exposure = j->value_float("exposure", cm.exposure);
+    cm.channel = j->value_u32("channel", cm.channel);
+}
+
 int config_from_json(const Json& p, const std::string& base_dir, ModuleConfig& c,
                      std::string& error) {
     if (!p.is_object()) {
@@ -308,6 +346,7 @@ int config_from_json(const Json& p, const std::string& base_dir, ModuleConfig& c
                   : conv == "directMulti" ? LENIA_CONV_DIRECT_MULTI
                                           : LENIA_CONV_DIRECT;
     c.fft_any_size = p.value_bool("fftAnySize", false);
+    colormap_from_json(p, c.colormap);
     const std::string prec = p.value_string("fftPrecision", "fp32");
     if (prec == "bf16x3") {
         c.fft_precision = LENIA_FFT_BF16X3;
@@ -957,6 +996,16 @@ lenia_frame_params LeniaModule::resolveFrameParams(const ParameterBus& bus, uint
 int LeniaModule::encode(uint32_t frame_index, uint32_t substeps, const ParameterBus& params,
                         cudaStream_t stream) {
     return step(resolveFrameParams(params, frame_index, audio_frame_), substeps, stream);
+}
+
+int LeniaModule::render(void* rgba16f, uint32_t dst_w, uint32_t dst_h, cudaStream_t s) {
+    if (!rgba16f || dst_w == 0 || dst_h == 0) return fail(LENIA_ERR_INVALID_ARG, "render: null buffer or empty size");
+    if (!field_[0]) return fail(LENIA_ERR_STATE, "render: module not set up");
+    const cudaError_t e = launch(LENIA_PHASE_COLORMAP, s, [&] {
+        return launch_colormap(field_[cur_], int(w_), int(h_), colormap_, rgba16f, int(dst_w), int(dst_h), s);
+    });
+    if (e != cudaSuccess) return cudaFail(e, "colour map");
+    return LENIA_OK;
 }
 
 int LeniaModule::initField(const lenia_frame_params&, cudaStream_t s) {

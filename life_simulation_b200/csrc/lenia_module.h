@@ -34,7 +34,17 @@ struct OrganismData {  // Lenia.cpp:137-145
 };
 
 // Everything setup() reads, after parsing (C struct or JSON).
+// The Lenia module's palette: ColorMapParams defaults
+// (LifeCore/Render/ColorMapPass.h:13-23) with Lenia's phases, channel and
+// scale (Lenia.cpp:349-354), then the params' "colorMap" block.
+ColorMapParams lenia_default_colormap();
+// ColorMapPass::configure's "colorMap" block (LifeCore/Render/ColorMapPass.cpp:
+// 70-101): "palette": "mono", "a"/"b"/"c"/"d" (3 numbers), "inputScale",
+// "inputBias", "exposure", "channel".
+void colormap_from_json(const Json& params, ColorMapParams& cm);
+
 struct ModuleConfig {
+    ColorMapParams colormap = lenia_default_colormap();
     uint32_t sim_width = 0, sim_height = 0;
     uint32_t conv_mode = LENIA_CONV_DIRECT;
     bool fft_any_size = false;
@@ -68,6 +78,7 @@ public:
     void configure(std::string instance, ModuleConfig cfg) {
         instance_ = std::move(instance);
         cfg_ = std::move(cfg);
+        colormap_ = cfg_.colormap;
     }
     // LeniaModule::setup (Lenia.cpp:208-408). Returns LENIA_OK,
     // LENIA_WARN_FALLBACK, or an error.
@@ -102,6 +113,11 @@ public:
     void info(lenia_info* out) const;
     const std::string& message() const { return message_; }
     const std::string& instance() const { return instance_; }
+    const ColorMapParams& colormap() const { return colormap_; }
+    void setColormap(const ColorMapParams& cm) { colormap_ = cm; }
+    // The colour map of the current field into a dst_w x dst_h RGBA16F
+    // device buffer (the module's outputField, Lenia.cpp:646-652).
+    int render(void* rgba16f, uint32_t dst_w, uint32_t dst_h, cudaStream_t stream);
     void setMessage(std::string m) { message_ = std::move(m); }
     cudaStream_t stream() const { return stream_; }
 
@@ -126,6 +142,7 @@ private:
     void release();
 
     std::string instance_ = "lenia0";
+    ColorMapParams colormap_ = lenia_default_colormap();
     ModuleConfig cfg_;
     std::string message_;
     std::vector<std::string> warnings_;

@@ -585,6 +585,7 @@ class RefLenia:
             L.ref_bus_value.argtypes = [P, ctypes.c_char_p, ctypes.c_float]
             L.ref_session_bus.restype = P
             L.ref_session_bus.argtypes = [P]
+            L.ref_colormap.argtypes = [P, u32, u32, P, P, u32, u32]
             cls._L = L
         return cls._L
 
@@ -650,3 +651,20 @@ class RefLenia:
 
     def pass_count(self) -> int:
         return int(self.lib().ref_pass_count(self.h_))
+
+
+def ref_colormap(field: np.ndarray, cm: dict, out_w: int, out_h: int) -> np.ndarray:
+    """The reference's colorMapField / colorMapFieldScaled (Shaders/Render/
+    ColorMap.metal, compiled for the CPU) on a float32 field: out_h x out_w x
+    4 floats, before the RGBA16F texture's rounding. cm: a, b, c, d (3 each),
+    inputScale, inputBias, exposure, channel."""
+    L = RefLenia.lib()
+    f = np.ascontiguousarray(field, np.float32)
+    h, w = f.shape
+    p = np.array(list(cm["a"]) + list(cm["b"]) + list(cm["c"]) + list(cm["d"])
+                 + [cm["inputScale"], cm["inputBias"], cm["exposure"]], np.float32)
+    params = np.concatenate([p, np.array([cm["channel"]], np.uint32).view(np.float32)])
+    out = np.empty((out_h, out_w, 4), np.float32)
+    if L.ref_colormap(_ptr(f), w, h, _ptr(params), _ptr(out), out_w, out_h) != 0:
+        raise RuntimeError("reference colour map kernel missing")
+    return out

@@ -4,7 +4,7 @@
 // TEST INFRASTRUCTURE ONLY (built into oracle/_ref/, never shipped, never on
 // the product path). The four shader files are included from the reference
 // tree at build time (the Makefile passes -I<reference root>); nothing of
-// them is copied into this repository. They are compiled in FP32, exactly as
+// them is copied into this repository. (Five files with ColorMap.metal.) They are compiled in FP32, exactly as
 // written, and every texel of a dispatch grid runs the kernel body once, in
 // parallel over rows (the kernels write only their own output texels, or, for
 // the FFT stages, the two autosort destinations that no other thread writes).
@@ -19,6 +19,8 @@
 //   realToComplex    Shaders/Common/FFT.metal:145-152
 //   complexToReal    Shaders/Common/FFT.metal:157-164
 //   clearR32F        Shaders/Common/FFT.metal:172-177
+//   colorMapField    Shaders/Render/ColorMap.metal:17-36
+//   colorMapFieldScaled Shaders/Render/ColorMap.metal:50-
 #include <metal_stdlib>
 
 #include <cstring>
@@ -29,6 +31,7 @@ namespace refmsl {
 #include "Shaders/Common/Random.metal"
 #include "Shaders/Common/FFT.metal"
 #include "Shaders/Field/Lenia.metal"
+#include "Shaders/Render/ColorMap.metal"
 }  // namespace refmsl
 
 #include "ref_kernels.h"
@@ -118,6 +121,17 @@ bool ref_dispatch(const std::string& fn, CpuImage* const* tex, const void* const
             grid2D(w, h, [&](uint2 g) { realToComplex(src, dst, p, g); });
         else
             grid2D(w, h, [&](uint2 g) { complexToReal(src, dst, p, g); });
+    } else if (fn == "colorMapField") {
+        const auto& p = as<ColorMapParams>(bytes[0], nbytes[0], "ColorMapParams");
+        RTex src(tex[0]);
+        WTex dst(tex[1]);
+        grid2D(w, h, [&](uint2 g) { colorMapField(src, dst, p, g); });
+    } else if (fn == "colorMapFieldScaled") {
+        const auto& p = as<ColorMapParams>(bytes[0], nbytes[0], "ColorMapParams");
+        const auto& sp = as<ColorMapScaledParams>(bytes[1], nbytes[1], "ColorMapScaledParams");
+        metal::texture2d<float, access::sample> src(tex[0]);
+        WTex dst(tex[1]);
+        grid2D(w, h, [&](uint2 g) { colorMapFieldScaled(src, dst, p, sp, g); });
     } else if (fn == "clearR32F") {
         const auto& p = as<FFTParams>(bytes[0], nbytes[0], "FFTParams");
         WTex dst(tex[0]);

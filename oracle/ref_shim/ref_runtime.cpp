@@ -493,6 +493,30 @@ void ref_bus_update(void* b, const RefFeaturesIn* f, float dt) {
     static_cast<life::ParameterBus*>(b)->update(m, dt);
 }
 
+// The reference's colour map kernels (Shaders/Render/ColorMap.metal) on a
+// w x h single-channel field into an ow x oh RGBA image (floats, before the
+// RGBA16F rounding of the texture): colorMapField when the sizes agree, else
+// colorMapFieldScaled, as ColorMapPass::encode / encodeScaled choose
+// (Lenia.cpp:646-652). cm: the 16 scalars of ColorMapParams in order.
+int ref_colormap(const float* field, uint32_t w, uint32_t h, const float* cm, float* rgba, uint32_t ow,
+                 uint32_t oh) {
+    std::vector<double> src(size_t(w) * h), dst(size_t(ow) * oh * 4);
+    for (size_t i = 0; i < src.size(); ++i) src[i] = field[i];
+    metal::CpuImage a{w, h, 1, src.data()}, b{ow, oh, 4, dst.data()};
+    metal::CpuImage* tex[2] = {&a, &b};
+    unsigned char params[16 * 4];
+    std::memcpy(params, cm, sizeof(params));
+    struct {
+        uint32_t w, h;
+    } sp{ow, oh};
+    const void* bytes[2] = {params, &sp};
+    const size_t nb[2] = {sizeof(params), sizeof(sp)};
+    const bool same = ow == w && oh == h;
+    if (!ref_dispatch(same ? "colorMapField" : "colorMapFieldScaled", tex, bytes, nb, ow, oh, 0, ~0u)) return -1;
+    for (size_t i = 0; i < dst.size(); ++i) rgba[i] = float(dst[i]);
+    return 0;
+}
+
 // The bus a Lenia session reads its parameters from (not to be destroyed).
 void* ref_session_bus(void* h) { return &static_cast<RefSession*>(h)->bus; }
 
