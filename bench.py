@@ -522,10 +522,11 @@ def run_sweep(args):
         b.upload(i, a)
     b.step(0)
     b.sync()
+    cm = lb.colormap_from_params({})
     t0 = time.perf_counter()
     for _ in range(4):
         b.step(60)
-        b.stats()  # synchronising activity readback
+        b.activity(cm)  # synchronising readback: the lab's luma activity per world
     batched_s = time.perf_counter() - t0
     paths = [b.path(i) for i in range(len(worlds))]
     b.close()

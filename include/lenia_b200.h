@@ -229,6 +229,30 @@ typedef struct lenia_profile_data {
 } lenia_profile_data;
 int lenia_profile(lenia_ctx* ctx, int enable);
 int lenia_profile_read(lenia_ctx* ctx, lenia_profile_data* out);
+/* ---- Colour map (the module's output layer) ----
+ * The field as an RGBA16F image through the module's cosine palette
+ * (Shaders/Render/ColorMap.metal: t = clamp(v * input_scale + input_bias,
+ * 0, 1), rgb = max(a + b cos(2 pi (c t + d)), 0) * exposure, alpha = t; v
+ * the channel `channel` of the field read as (A, 0, 0, 1)). The palette is
+ * the reference Lenia module's (ColorMapPass defaults with d = (0.60, 0.45,
+ * 0.30), channel 0, Lenia.cpp:349-354) updated by the params' "colorMap"
+ * block (ColorMapPass.cpp:70-101). */
+typedef struct lenia_colormap {
+    float a[3], b[3], c[3], d[3];
+    float input_scale, input_bias, exposure;
+    uint32_t channel;
+} lenia_colormap;
+int lenia_get_colormap(lenia_ctx* ctx, lenia_colormap* out);
+int lenia_set_colormap(lenia_ctx* ctx, const lenia_colormap* cm);
+/* The palette a params JSON object gives (host only, no device). */
+int lenia_colormap_from_json(const char* params_json, lenia_colormap* out);
+/* The current field's colour layer into `dst` (device, width x height
+ * pixels of 4 halves, RGBA): colorMapField when the size is the field's,
+ * else colorMapFieldScaled (bilinear, wrapping, at output pixel centres) --
+ * the module's output at the scene resolution (Lenia.cpp:646-652).
+ * Asynchronous on `stream` after the queued steps. */
+int lenia_render_rgba16f(lenia_ctx* ctx, void* dst, uint32_t width, uint32_t height, void* stream);
+
 /* ---- Many worlds at once (batched sweep) ----
  * Replaces the reference's one-world-at-a-time variant loop
  * (Apps/LifePresetLab/main.cpp:718-795, a SceneRunner per variant): n
@@ -263,6 +287,15 @@ int lenia_batch_step(lenia_batch* b, uint32_t steps, void* stream);
 int lenia_batch_stats(lenia_batch* b, double* mean, double* var);
 /* LENIA_CONV_DIRECT or LENIA_CONV_FFT: the path the batch gave a world. */
 int lenia_batch_world_path(lenia_batch* b, uint32_t world, uint32_t* path);
+/* The reference Lenia module's noise init (leniaInit, Lenia.metal:43-61) of
+ * one world on the device, from reset seed `seed` (deriveSeed(seed, "LEN1"),
+ * Lenia.cpp:448-451) with initCoverage / initScale. */
+int lenia_batch_init_noise(lenia_batch* b, uint32_t world, uint32_t seed, float init_coverage, float init_scale);
+/* Activity of every world as the sweep runner measures it
+ * (Apps/LifePresetLab/main.cpp:61-82): mean and standard deviation of the
+ * luma 0.2126 R + 0.7152 G + 0.0722 B of the world's RGBA16F colour layer
+ * through palette `cm` (n doubles each). */
+int lenia_batch_activity(lenia_batch* b, const lenia_colormap* cm, double* mean_luma, double* stddev_luma);
 int lenia_batch_sync(lenia_batch* b);
 const char* lenia_batch_last_message(lenia_batch* b);
 
@@ -357,29 +390,6 @@ int lenia_adjoint_backward(lenia_adjoint* a, const float* g_final, float* g_init
 int lenia_adjoint_stats(lenia_adjoint* a, uint64_t* device_bytes, uint64_t* launches);
 const char* lenia_adjoint_last_message(lenia_adjoint* a);
 
-/* ---- Colour map (the module's output layer) ----
- * The field as an RGBA16F image through the module's cosine palette
- * (Shaders/Render/ColorMap.metal: t = clamp(v * input_scale + input_bias,
- * 0, 1), rgb = max(a + b cos(2 pi (c t + d)), 0) * exposure, alpha = t; v
- * the channel `channel` of the field read as (A, 0, 0, 1)). The palette is
- * the reference Lenia module's (ColorMapPass defaults with d = (0.60, 0.45,
- * 0.30), channel 0, Lenia.cpp:349-354) updated by the params' "colorMap"
- * block (ColorMapPass.cpp:70-101). */
-typedef struct lenia_colormap {
-    float a[3], b[3], c[3], d[3];
-    float input_scale, input_bias, exposure;
-    uint32_t channel;
-} lenia_colormap;
-int lenia_get_colormap(lenia_ctx* ctx, lenia_colormap* out);
-int lenia_set_colormap(lenia_ctx* ctx, const lenia_colormap* cm);
-/* The palette a params JSON object gives (host only, no device). */
-int lenia_colormap_from_json(const char* params_json, lenia_colormap* out);
-/* The current field's colour layer into `dst` (device, width x height
- * pixels of 4 halves, RGBA): colorMapField when the size is the field's,
- * else colorMapFieldScaled (bilinear, wrapping, at output pixel centres) --
- * the module's output at the scene resolution (Lenia.cpp:646-652).
- * Asynchronous on `stream` after the queued steps. */
-int lenia_render_rgba16f(lenia_ctx* ctx, void* dst, uint32_t width, uint32_t height, void* stream);
 
 /* ---- Parameter bus and scenes ----
  * The reference's ParameterBus (LifeCore/Params/ParameterBus.{h,cpp}) and

@@ -104,6 +104,7 @@ EXPORTS = (
     "lenia_bus_set_section", "lenia_bus_clear_features", "lenia_bus_update", "lenia_bus_value",
     "lenia_bus_last_message", "lenia_create_scene_module", "lenia_attach_bus",
     "lenia_get_colormap", "lenia_set_colormap", "lenia_colormap_from_json", "lenia_render_rgba16f",
+    "lenia_batch_init_noise", "lenia_batch_activity",
 )
 
 
@@ -243,6 +244,8 @@ def load_library(path: str = LIB_PATH):
     L.lenia_set_colormap.argtypes = [P, ctypes.POINTER(ColorMap)]
     L.lenia_colormap_from_json.argtypes = [ctypes.c_char_p, ctypes.POINTER(ColorMap)]
     L.lenia_render_rgba16f.argtypes = [P, P, u32, u32, P]
+    L.lenia_batch_init_noise.argtypes = [P, u32, u32, ctypes.c_float, ctypes.c_float]
+    L.lenia_batch_activity.argtypes = [P, ctypes.POINTER(ColorMap), P, P]
     for name in EXPORTS:
         getattr(L, name)  # raises AttributeError if the build lacks a symbol
     _LIB = L
@@ -548,6 +551,19 @@ class LeniaBatch:
         self._check(self._L.lenia_batch_stats(self._h, mean.ctypes.data_as(ctypes.c_void_p),
                                               var.ctypes.data_as(ctypes.c_void_p)))
         return mean, var
+
+    def init_noise(self, i: int, seed: int, coverage: float = 0.4, scale: float = 24.0) -> None:
+        """The reference module's noise init of world i (reset seed `seed`)."""
+        self._check(self._L.lenia_batch_init_noise(self._h, i, seed, coverage, scale))
+
+    def activity(self, cm: "ColorMap"):
+        """Per-world mean and standard deviation of the colour layer's luma."""
+        n = len(self.worlds)
+        mean = np.empty(n, np.float64)
+        std = np.empty(n, np.float64)
+        self._check(self._L.lenia_batch_activity(self._h, ctypes.byref(cm), mean.ctypes.data_as(ctypes.c_void_p),
+                                                 std.ctypes.data_as(ctypes.c_void_p)))
+        return mean, std
 
     def path(self, i: int) -> int:
         p = ctypes.c_uint32()

@@ -26,6 +26,7 @@
 #include <vector>
 
 #include "../../include/lenia_b200.h"
+#include "colormap.cuh"
 #include "lenia_device.cuh"
 #include "lenia_kernels.h"
 #include "lenia_module.h"
@@ -61,6 +62,33 @@ __global__ void stats_kernel(const float* const* fields, const int* npx, double*
         const double v = double(f[i]);
         s += v;
         s2 += v * v;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        s += __shfl_down_sync(0xffffffffu, s, o);
+        s2 += __shfl_down_sync(0xffffffffu, s2, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(out + 2 * w, s);
+        atomicAdd(out + 2 * w + 1, s2);
+    }
+}
+
+// Per-world luma statistics of the colour layer (Apps/LifePresetLab/
+// main.cpp:61-82): each pixel's RGBA16F palette texel, luma 0.2126 R +
+// 0.7152 G + 0.0722 B of the halves in double; sum and sum of squares.
+__global__ void activity_kernel(const float* const* fields, const int* npx, ColorMapParams cm, double* out, int n) {
+    const int w = blockIdx.y;
+    if (w >= n) return;
+    const float* f = fields[w];
+    const int count = npx[w];
+    double s = 0.0, s2 = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        __half px[4];
+        palette_rgba16f(cm, channel_of(f[i], cm.channel), px);
+        const double l = 0.2126 * double(__half2float(px[0])) + 0.7152 * double(__half2float(px[1])) +
+                         0.0722 * double(__half2float(px[2]));
+        s += l;
+        s2 += l * l;
     }
     for (int o = 16; o > 0; o >>= 1) {
         s += __shfl_down_sync(0xffffffffu, s, o);
@@ -692,6 +720,43 @@ int lenia_batch_stats(lenia_batch* bb, double* mean, double* var) {
         var[i] = std::max(0.0, h[2 * size_t(i) + 1] / cnt - mean[i] * mean[i]);
     }
     return LENIA_OK;
+}
+
+int lenia_batch_activity(lenia_batch* bb, const lenia_colormap* cm, double* mean_luma, double* stddev_luma) {
+    if (!bb || !cm || !mean_luma || !stddev_luma) return LENIA_ERR_INVALID_ARG;
+    BatchContext& b = bb->ctx;
+    const int n = int(b.worlds.size());
+    static_assert(sizeof(lenia_colormap) == sizeof(lenia::ColorMapParams), "colour map layout");
+    lenia::ColorMapParams p;
+    std::memcpy(&p, cm, sizeof(p));
+    cudaError_t e = cudaMemsetAsync(b.d_stats, 0, sizeof(double) * 2 * n, b.stream);
+    if (e == cudaSuccess) {
+        lenia::activity_kernel<<<dim3(16, unsigned(n)), 256, 0, b.stream>>>(b.d_field_ptrs[b.cur], b.d_npx, p,
+                                                                            b.d_stats, n);
+        e = cudaGetLastError();
+    }
+    std::vector<double> h(2 * size_t(n));
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemcpy(h.data(), b.d_stats, h.size() * sizeof(double), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return b.fail(LENIA_ERR_CUDA, cudaGetErrorString(e));
+    for (int i = 0; i < n; ++i) {
+        const double cnt = double(b.worlds[size_t(i)].width) * b.worlds[size_t(i)].height;
+        const double mean = h[2 * size_t(i)] / cnt;
+        mean_luma[i] = mean;
+        stddev_luma[i] = std::sqrt(std::max(0.0, h[2 * size_t(i) + 1] / cnt - mean * mean));
+    }
+    return LENIA_OK;
+}
+
+int lenia_batch_init_noise(lenia_batch* bb, uint32_t world, uint32_t seed, float init_coverage, float init_scale) {
+    if (!bb || world >= bb->ctx.worlds.size()) return LENIA_ERR_INVALID_ARG;
+    BatchContext& b = bb->ctx;
+    const lenia_world& w = b.worlds[world];
+    const lenia::InitParams ip{init_coverage, init_scale, lenia::derive_seed(seed, 0x4C454E31u), w.width, w.height};
+    cudaError_t e = lenia::launch_init_noise(b.field(int(world), b.cur), ip, b.stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b.stream);
+    b.spectra_valid = false;
+    return e == cudaSuccess ? LENIA_OK : b.fail(LENIA_ERR_CUDA, cudaGetErrorString(e));
 }
 
 int lenia_batch_world_path(lenia_batch* bb, uint32_t world, uint32_t* path) {

@@ -10,14 +10,11 @@
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
+#include "colormap.cuh"
 #include "lenia_kernels.h"
 
 namespace lenia {
 namespace {
-
-__device__ __forceinline__ float channel_of(float r, uint32_t ch) {
-    return ch == 0u ? r : ch >= 3u ? 1.0f : 0.0f;
-}
 
 __global__ void colormap_kernel(const float* __restrict__ field, int w, int h, ColorMapParams p,
                                 ushort4* __restrict__ out, int ow, int oh) {
@@ -45,19 +42,10 @@ __global__ void colormap_kernel(const float* __restrict__ field, int w, int h, C
         const float bot = __fadd_rn(t01, __fmul_rn(t11 - t01, ax));
         v = __fadd_rn(top, __fmul_rn(bot - top, ay));
     }
-    float t = __fadd_rn(__fmul_rn(v, p.input_scale), p.input_bias);
-    t = fminf(fmaxf(t, 0.0f), 1.0f);
-    float rgb[3];
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-        // __fmul_rn / __fadd_rn: no contraction, the palette's own rounding.
-        const float phase = __fmul_rn(6.28318530718f, __fadd_rn(__fmul_rn(p.c[i], t), p.d[i]));
-        rgb[i] = __fmul_rn(fmaxf(__fadd_rn(p.a[i], __fmul_rn(p.b[i], cosf(phase))), 0.0f), p.exposure);
-    }
-    out[size_t(y) * ow + x] = make_ushort4(__half_as_ushort(__float2half_rn(rgb[0])),
-                                           __half_as_ushort(__float2half_rn(rgb[1])),
-                                           __half_as_ushort(__float2half_rn(rgb[2])),
-                                           __half_as_ushort(__float2half_rn(t)));
+    __half rgba[4];
+    palette_rgba16f(p, v, rgba);
+    out[size_t(y) * ow + x] = make_ushort4(__half_as_ushort(rgba[0]), __half_as_ushort(rgba[1]),
+                                           __half_as_ushort(rgba[2]), __half_as_ushort(rgba[3]));
 }
 
 }  // namespace
