@@ -391,6 +391,22 @@ int lenia_adjoint_stats(lenia_adjoint* a, uint64_t* device_bytes, uint64_t* laun
 const char* lenia_adjoint_last_message(lenia_adjoint* a);
 
 
+/* ---- State files (.npy) ----
+ * NumPy .npy v1.0, float32, C order (LifeCore/IO/NpyWriter.h:15-31): the
+ * reference's state exchange format. Reading requires the caller's shape:
+ * the payload is sized from it, never from the file, and a bad magic, a
+ * truncated header or payload, another dtype, a Fortran-order array or a
+ * different shape is an error (LENIA_ERR_PARSE; nothing is written to `out`
+ * beyond a complete read). Host only. lenia_last_message(NULL) says why a
+ * call on this thread failed. */
+int lenia_npy_write_f32(const char* path, const float* data, size_t count, const uint32_t* shape, uint32_t ndim);
+int lenia_npy_read_f32(const char* path, const uint32_t* shape, uint32_t ndim, float* out, size_t count);
+/* The field as (sim_height, sim_width) float32 (SimulationModule::dumpState /
+ * loadState, LifeCore/Sim/SimulationModule.h:48-78). Loading replaces the
+ * field and counts as the init (the next encode does not re-initialise). */
+int lenia_save_state(lenia_ctx* ctx, const char* path);
+int lenia_load_state(lenia_ctx* ctx, const char* path);
+
 /* ---- Parameter bus and scenes ----
  * The reference's ParameterBus (LifeCore/Params/ParameterBus.{h,cpp}) and
  * scene loader (LifeCore/Params/Scene.cpp): a table of "<module>.<param>"

@@ -105,6 +105,7 @@ EXPORTS = (
     "lenia_bus_last_message", "lenia_create_scene_module", "lenia_attach_bus",
     "lenia_get_colormap", "lenia_set_colormap", "lenia_colormap_from_json", "lenia_render_rgba16f",
     "lenia_batch_init_noise", "lenia_batch_activity",
+    "lenia_npy_write_f32", "lenia_npy_read_f32", "lenia_save_state", "lenia_load_state",
 )
 
 
@@ -245,6 +246,10 @@ def load_library(path: str = LIB_PATH):
     L.lenia_colormap_from_json.argtypes = [ctypes.c_char_p, ctypes.POINTER(ColorMap)]
     L.lenia_render_rgba16f.argtypes = [P, P, u32, u32, P]
     L.lenia_batch_init_noise.argtypes = [P, u32, u32, ctypes.c_float, ctypes.c_float]
+    L.lenia_npy_write_f32.argtypes = [ctypes.c_char_p, P, ctypes.c_size_t, P, u32]
+    L.lenia_npy_read_f32.argtypes = [ctypes.c_char_p, P, u32, P, ctypes.c_size_t]
+    L.lenia_save_state.argtypes = [P, ctypes.c_char_p]
+    L.lenia_load_state.argtypes = [P, ctypes.c_char_p]
     L.lenia_batch_activity.argtypes = [P, ctypes.POINTER(ColorMap), P, P]
     for name in EXPORTS:
         getattr(L, name)  # raises AttributeError if the build lacks a symbol
@@ -416,6 +421,14 @@ class LeniaModule:
         """Colour layer (RGBA16F, 8 bytes per pixel) into a device buffer."""
         self._check(self._L.lenia_render_rgba16f(self._h, ctypes.c_void_p(ptr), width, height,
                                                  ctypes.c_void_p(stream) if stream else None))
+
+    def save_state(self, path: str) -> None:
+        """The field as a (height, width) float32 .npy file."""
+        self._check(self._L.lenia_save_state(self._h, os.fsencode(path)))
+
+    def load_state(self, path: str) -> None:
+        """Replace the field from a (height, width) float32 .npy file."""
+        self._check(self._L.lenia_load_state(self._h, os.fsencode(path)))
 
     def attach_bus(self, bus) -> None:
         """Read per-frame parameters from a shared ParamBus (None: own bus)."""
@@ -790,3 +803,26 @@ def colormap_from_params(params) -> ColorMap:
     if rc < 0:
         raise LeniaError(rc, L.lenia_last_message(None).decode(errors="replace"))
     return cm
+
+
+def npy_write(path: str, a: np.ndarray) -> None:
+    """A float32 array as a .npy v1.0 file (C order), by the library's writer."""
+    L = load_library()
+    a = np.ascontiguousarray(a, np.float32)
+    shape = np.array(a.shape, np.uint32)
+    rc = L.lenia_npy_write_f32(os.fsencode(path), a.ctypes.data_as(ctypes.c_void_p), a.size,
+                               shape.ctypes.data_as(ctypes.c_void_p), a.ndim)
+    if rc < 0:
+        raise LeniaError(rc, L.lenia_last_message(None).decode(errors="replace"))
+
+
+def npy_read(path: str, shape) -> np.ndarray:
+    """A float32 .npy file that must have `shape`, by the library's reader."""
+    L = load_library()
+    shp = np.array(list(shape), np.uint32)
+    out = np.empty(tuple(int(x) for x in shape), np.float32)
+    rc = L.lenia_npy_read_f32(os.fsencode(path), shp.ctypes.data_as(ctypes.c_void_p), shp.size,
+                              out.ctypes.data_as(ctypes.c_void_p), out.size)
+    if rc < 0:
+        raise LeniaError(rc, L.lenia_last_message(None).decode(errors="replace"))
+    return out

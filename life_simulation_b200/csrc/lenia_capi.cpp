@@ -9,6 +9,7 @@
 
 #include "../../include/lenia_b200.h"
 #include "lenia_module.h"
+#include "npy_io.h"
 
 struct lenia_ctx {
     lenia::LeniaModule module;
@@ -392,6 +393,75 @@ int lenia_render_rgba16f(lenia_ctx* c, void* dst, uint32_t width, uint32_t heigh
         cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c->module.stream();
         return set_msg(c, c->module.render(dst, width, height, s));
     });
+}
+
+// ---------------------------------------------------------- state files
+
+int lenia_npy_write_f32(const char* path, const float* data, size_t count, const uint32_t* shape, uint32_t ndim) {
+    if (!path || (!shape && ndim)) return LENIA_ERR_INVALID_ARG;
+    return guarded(nullptr, [&] {
+        std::string err;
+        if (!lenia::write_npy_f32(path, data, count, std::vector<uint32_t>(shape, shape + ndim), err)) {
+            g_create_error = err;
+            return int(LENIA_ERR_PARSE);
+        }
+        return int(LENIA_OK);
+    });
+}
+
+int lenia_npy_read_f32(const char* path, const uint32_t* shape, uint32_t ndim, float* out, size_t count) {
+    if (!path || !shape || !out) return LENIA_ERR_INVALID_ARG;
+    return guarded(nullptr, [&] {
+        std::string err;
+        const std::vector<uint32_t> expected(shape, shape + ndim);
+        size_t n = 1;
+        for (uint32_t s : expected) n *= s;
+        if (n != count) {
+            g_create_error = "npy read: the expected shape does not hold `count` values";
+            return int(LENIA_ERR_INVALID_ARG);
+        }
+        std::vector<float> data;
+        if (!lenia::read_npy_f32(path, expected, data, err)) {
+            g_create_error = err;
+            return int(LENIA_ERR_PARSE);
+        }
+        std::memcpy(out, data.data(), n * sizeof(float));
+        return int(LENIA_OK);
+    });
+}
+
+int lenia_save_state(lenia_ctx* c, const char* path) {
+    if (!c || !path) return LENIA_ERR_INVALID_ARG;
+    uint32_t w = 0, h = 0;
+    lenia_field_size(c, &w, &h);
+    std::vector<float> host(size_t(w) * h);
+    int rc = lenia_download(c, host.data(), host.size());
+    if (rc < 0) return rc;
+    return guarded(c, [&] {
+        std::string err;
+        if (!lenia::write_npy_f32(path, host.data(), host.size(), {h, w}, err)) {
+            c->message = err;
+            return int(LENIA_ERR_PARSE);
+        }
+        return int(LENIA_OK);
+    });
+}
+
+int lenia_load_state(lenia_ctx* c, const char* path) {
+    if (!c || !path) return LENIA_ERR_INVALID_ARG;
+    uint32_t w = 0, h = 0;
+    lenia_field_size(c, &w, &h);
+    std::vector<float> host;
+    const int rc = guarded(c, [&] {
+        std::string err;
+        if (!lenia::read_npy_f32(path, {h, w}, host, err)) {
+            c->message = err;
+            return int(LENIA_ERR_PARSE);
+        }
+        return int(LENIA_OK);
+    });
+    if (rc < 0) return rc;
+    return lenia_upload(c, host.data(), host.size());
 }
 
 // ---------------------------------------------------------------- the bus

@@ -586,6 +586,10 @@ class RefLenia:
             L.ref_session_bus.restype = P
             L.ref_session_bus.argtypes = [P]
             L.ref_colormap.argtypes = [P, u32, u32, P, P, u32, u32]
+            L.ref_npy_write.argtypes = [ctypes.c_char_p, P, ctypes.c_size_t, P, u32, ctypes.c_char_p,
+                                        ctypes.c_size_t]
+            L.ref_npy_read.argtypes = [ctypes.c_char_p, P, u32, P, ctypes.c_size_t, ctypes.c_char_p,
+                                       ctypes.c_size_t]
             cls._L = L
         return cls._L
 
@@ -667,4 +671,25 @@ def ref_colormap(field: np.ndarray, cm: dict, out_w: int, out_h: int) -> np.ndar
     out = np.empty((out_h, out_w, 4), np.float32)
     if L.ref_colormap(_ptr(f), w, h, _ptr(params), _ptr(out), out_w, out_h) != 0:
         raise RuntimeError("reference colour map kernel missing")
+    return out
+
+
+def ref_npy_write(path: str, a: np.ndarray) -> None:
+    """The reference's writeNPYFloat32 (LifeCore/IO/NpyWriter.cpp)."""
+    L = RefLenia.lib()
+    a = np.ascontiguousarray(a, np.float32)
+    shape = np.array(a.shape, np.uint32)
+    err = ctypes.create_string_buffer(512)
+    if L.ref_npy_write(os.fsencode(path), _ptr(a), a.size, _ptr(shape), a.ndim, err, 512) != 0:
+        raise ValueError(err.value.decode())
+
+
+def ref_npy_read(path: str, shape) -> np.ndarray:
+    """The reference's readNPYFloat32 with an expected shape."""
+    L = RefLenia.lib()
+    shp = np.array(list(shape), np.uint32)
+    out = np.empty(tuple(int(x) for x in shape), np.float32)
+    err = ctypes.create_string_buffer(512)
+    if L.ref_npy_read(os.fsencode(path), _ptr(shp), shp.size, _ptr(out), out.size, err, 512) != 0:
+        raise ValueError(err.value.decode() or "read failed")
     return out

@@ -19,6 +19,7 @@
 // updateCPU(audio) and encode(ctx) once per frame.
 #include "LifeCore/Metal/CommandGraph.h"
 #include "LifeCore/Metal/ResourcePool.h"
+#include "LifeCore/IO/NpyWriter.h"
 #include "LifeCore/Params/ParameterBus.h"
 #include "LifeCore/Params/Scene.h"
 #include "LifeCore/Render/ColorMapPass.h"
@@ -514,6 +515,30 @@ int ref_colormap(const float* field, uint32_t w, uint32_t h, const float* cm, fl
     const bool same = ow == w && oh == h;
     if (!ref_dispatch(same ? "colorMapField" : "colorMapFieldScaled", tex, bytes, nb, ow, oh, 0, ~0u)) return -1;
     for (size_t i = 0; i < dst.size(); ++i) rgba[i] = float(dst[i]);
+    return 0;
+}
+
+// The reference's .npy writer and reader (LifeCore/IO/NpyWriter.cpp); 0 or
+// -1 with the message in err.
+int ref_npy_write(const char* path, const float* data, size_t count, const uint32_t* shape, uint32_t ndim, char* err,
+                  size_t err_n) {
+    std::string e;
+    if (!life::writeNPYFloat32(path, data, count, std::vector<uint32_t>(shape, shape + ndim), e)) {
+        std::snprintf(err, err_n, "%s", e.c_str());
+        return -1;
+    }
+    return 0;
+}
+int ref_npy_read(const char* path, const uint32_t* shape, uint32_t ndim, float* out, size_t count, char* err,
+                 size_t err_n) {
+    std::string e;
+    std::vector<float> data;
+    if (!life::readNPYFloat32(path, std::vector<uint32_t>(shape, shape + ndim), data, e)) {
+        std::snprintf(err, err_n, "%s", e.c_str());
+        return -1;
+    }
+    if (data.size() != count) return -1;
+    std::memcpy(out, data.data(), count * sizeof(float));
     return 0;
 }
 
