@@ -50,9 +50,9 @@ METRIC = "Lenia Mpixel-steps/s (FFT, 3 kernels, 1080p)"
 UNIT = "Mpixel-steps/s"
 WORKLOAD = "fft3_1080p"
 FALLBACK_HBM_GBS = 6650.0
-# dram__bytes_read.sum + dram__bytes_write.sum per launch of the dominant
-# kernel from one ncu capture (profiles/), None until captured.
-NCU_TRAFFIC_BYTES = {}
+# dram__bytes_read.sum + dram__bytes_write.sum per launch from one ncu
+# capture of the default workload (profiles/lenia_fft_step_1080p_k3.md).
+NCU_TRAFFIC_BYTES = {"row_growth": 33_256_704 + 5_632, "column": 14_575_104 + 5_376}
 
 
 def parse_args():
