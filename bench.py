@@ -20,8 +20,8 @@ pixels x steps; ``value`` is whole-job Mpixel-steps/s.
   against the measured copy bandwidth in MEASURED_PEAKS.json.
 * cpu_baseline: the reference's own Lenia module and kernels compiled for
   the CPU (oracle/_ref), on a bounded row band of the same workload.
-* adjoint: the gradient form on 32 worlds of 512x512 (K=2, R=16, T=64,
-  checkpoints every 8): device time of the forward rollout and of the
+* adjoint: the gradient form on 32 worlds of 512x512 (K=2, R=16, growth
+  mode 1, T=64, checkpoints every 8): device time of the forward rollout and of the
   backward (recomputation included), CUDA events on the launching stream
   with an L2 flush before each; ratio = backward / forward.
 * tc: 4096x4096, 3 kernels R=32, 64 steps per arithmetic of the column DFT
@@ -410,7 +410,7 @@ def adjoint_bench(reps: int = 5, warmup: int = 3) -> dict:
     eng.close()
     f, b = statistics.median(fwd), statistics.median(bwd)
     px_steps = B * W * H * T
-    return {"workload": "adjoint_512: 32 worlds 512x512, K=2 R=16 b=[1],[0.5,1], T=64, checkpoints every 8",
+    return {"workload": "adjoint_512: 32 worlds 512x512, K=2 R=16 b=[1],[0.5,1], growth mode 1, T=64, checkpoints every 8",
             "forward_ms": f, "backward_ms": b, "ratio": b / f,
             "forward_mpx_steps_s": px_steps / (f / 1e3) / 1e6,
             "backward_mpx_steps_s": px_steps / (b / 1e3) / 1e6,
@@ -424,7 +424,7 @@ def run_adjoint(args):
 
     torch.cuda.set_device(0)
     r = adjoint_bench(args.adjoint_reps)
-    line = {"metric": "Lenia adjoint/forward time ratio (32 x 512x512, K=2, R=16, T=64, checkpoints every 8)",
+    line = {"metric": "Lenia adjoint/forward time ratio (32 x 512x512, K=2, R=16, growth mode 1, T=64, checkpoints every 8)",
             "value": r["ratio"], "unit": "x", "higher_is_better": False, "n_gpus": 1, "dtype": "f32",
             "data": "synthetic", "config": {"workload": r["workload"]}}
     line.update(r)

@@ -254,8 +254,8 @@ inline dim3 world_grid(int per_sm, int groups, int n) {
 #define LENIA_ROW_PLANS(X)     \
     X(960, Plan<8, 15, 8>)     \
     X(512, Plan<8, 8, 8>)      \
-    X(2048, Plan<16, 8, 16>)   \
-    X(256, Plan<16, 16>)       \
+    X(2048, Plan<16, 16, 8>)   \
+    X(256, Plan<8, 4, 8>)      \
     X(192, Plan<8, 3, 8>)      \
     X(128, Plan<16, 8>)        \
     X(64, Plan<8, 8>)

@@ -20,12 +20,12 @@
 //
 // Per backward step, two launches mirror the forward's two:
 //   row pass: inverse row FFT of the previous column pass's output -> dL/dA_{t+1};
-//     clip mask -> g; inverse row FFTs of the stored potential spectra of step t
-//     -> U_k -> q_k and the parameter sums; forward row FFTs of q_k.
+//     clip mask -> g; the potentials U_k of step t (kept as planes by the
+//     forward row pass) -> q_k and the parameter sums; forward row FFTs of q_k.
 //   column pass: column FFTs of q_k, sum_k K^_k Q_k (and the beta sums against
 //     the column FFT of A_t's row spectrum), one inverse column FFT.
-// The forward keeps the potential spectra, row spectra and fields of the
-// current segment of `checkpoint_every` steps and A at every checkpoint; the
+// The forward keeps the potentials, row spectra and fields of the current
+// segment of `checkpoint_every` steps and A at every checkpoint; the
 // backward recomputes each earlier segment from its checkpoint with the
 // forward kernels (bit-identical), then runs the segment's adjoint steps.
 #include <cuda_runtime.h>
@@ -57,7 +57,7 @@ struct AdjRowWorld {
     const float* g_in;    // with SG: dL/dpre_{t+1}; without: dL/dA_{t+1}
     const float* A_next;  // A_{t+1}: clip mask of step t
     const float* A_cur;   // A_t (growth mode 1's dt term)
-    const float2* U;      // nk potential spectra of step t; null: only write dL/dA_{t+1}
+    const float* U;       // nk potential planes (H x W) of step t; null: only write dL/dA_{t+1}
     float* g_out;         // dL/dpre_t
     float2* SQ;           // nk row spectra of q_k
     float* gA_out;        // dL/dA_{t+1} when U is null
@@ -92,14 +92,17 @@ using fft::csub;
 using namespace fftct;
 using namespace fastfft;
 
-__device__ __forceinline__ float warp_sum(float v) {
+__device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     return v;
 }
 // Adds every thread's v into a shared FP64 accumulator, one atomic per warp.
-// All threads of the block call it.
-__device__ __forceinline__ void block_add(double* red, float v) {
+// All threads of the block call it. The per-thread partial sums are FP64 as
+// well: which pixels a thread sums depends on the tuned rows or columns per
+// CTA, so only FP64 keeps the parameter gradients independent of the tuning
+// (up to the order of FP64 additions).
+__device__ __forceinline__ void block_add(double* red, double v) {
     v = warp_sum(v);
     if ((threadIdx.x & 31u) == 0u) atomicAdd(red, double(v));
 }
@@ -135,7 +138,7 @@ __global__ void __launch_bounds__(RowK<PI, RB>::T, (512 / RowK<PI, RB>::T > 1 ? 
     const float inv_sw = sw_ok ? 1.0f / p.sum_weights : 0.0f;
     const float dt = p.dt, ca = a.ca;
     const bool has_q = sw.U != nullptr;
-    float pdt = 0.0f, pcommon = 0.0f;
+    double pdt = 0.0, pcommon = 0.0;
     for (int y0 = blockIdx.x * RB; y0 < H; y0 += gridDim.x * RB) {
         const int rows = min(RB, H - y0);
         int jj[ITL], bi[ITL];
@@ -206,28 +209,21 @@ __global__ void __launch_bounds__(RowK<PI, RB>::T, (512 / RowK<PI, RB>::T > 1 ? 
         // The dt and mode-1 terms are linear in the kernels' contributions,
         // so they are summed kernel by kernel (no per-pixel accumulator).
         for (int kk = 0; kk < nk; ++kk) {
-            stage_rows<M, RB, T, PITCH>(ba, sw.U + size_t(kk) * M * H, H, y0, rows);
-            cp_async_wait_all();
-            __syncthreads();
-            pass_gen<PI, 0, true, RB, T>([&](int b, int i) { return c2r_split<M>(ba + b * PITCH, twr, i); },
-                                         [&](int b, int i, float2 v) { bb[b * PITCH + i] = v; }, twi, rows);
-            __syncthreads();
-            float2* X = mid_passes<PI, 1, PI::np - 1, true, RB, T, PITCH>(bb, ba, twi, rows);
+            // The potentials of step t, kept by the recomputation's row pass.
+            const float* Uk = sw.U + size_t(kk) * H * W;
             const auto pick = [&](const float(&v)[kMaxKernels]) {
                 return kk == 0 ? v[0] : kk == 1 ? v[1] : kk == 2 ? v[2] : v[3];
             };
             const float mu = pick(p.mu), inv_sigma = 1.0f / pick(p.sigma), hw = pick(p.weight);
             const float coef = asym ? (sw_ok ? dt * hw * inv_sw : 0.0f) : 2.0f * dt * hw;
-            float pmu = 0.0f, psig = 0.0f, ph = 0.0f;
+            double pmu = 0.0, psig = 0.0, ph = 0.0;
             float2 zq[ITL][RC];
 #pragma unroll
             for (int it = 0; it < ITL; ++it) {
                 if (!ok[it]) continue;
                 float2 z[RC];
 #pragma unroll
-                for (int t = 0; t < RC; ++t) z[t] = X[bi[it] * PITCH + IL::in(jj[it], t)];
-                IL::template twiddle<true>(z, jj[it], twi);
-                Dft<RC, true>::run(z);
+                for (int t = 0; t < RC; ++t) z[t] = __ldg(reinterpret_cast<const float2*>(Uk + gidx(it, t)));
 #pragma unroll
                 for (int t = 0; t < RC; ++t) {
                     float qv[2];
@@ -258,8 +254,8 @@ __global__ void __launch_bounds__(RowK<PI, RB>::T, (512 / RowK<PI, RB>::T > 1 ? 
             block_add(&red[kk * kPerKernel + 0], pmu);
             block_add(&red[kk * kPerKernel + 1], psig);
             block_add(&red[kk * kPerKernel + 2], ph);
-            __syncthreads();  // X read; the buffers are free again
-            // Forward row transform of q_k: first pass (radix RC) from registers.
+            // (The shared buffers are free: the last reader of them was
+            // followed by a barrier.) Forward row transform of q_k: first pass (radix RC) from registers.
 #pragma unroll
             for (int it = 0; it < ITL; ++it) {
                 if (!ok[it]) continue;
@@ -406,7 +402,7 @@ __global__ void __launch_bounds__(ColK<PF, B>::T)
                 for (int tb = 0; tb < a.ntab; ++tb) {
                     if (a.tab_kernel[tb] != kk) continue;
                     const float* dtb = a.dtab + size_t(tb) * (M + 1) * Hh;
-                    float part = 0.0f;
+                    double part = 0.0;
 #pragma unroll
                     for (int it = 0; it < ITL; ++it) {
                         if (!ok[it]) continue;
@@ -466,58 +462,70 @@ __global__ void finalize_kernel(const double* __restrict__ acc, double* __restri
 
 // ---------------------------------------------------------------- dispatch
 
-constexpr int adj_col_batch(int nrl) { return 4 * nrl <= 576 ? 4 : 2; }
-constexpr int adj_row_batch(int nrc) { return 128 / nrc >= 4 ? 4 : 128 / nrc >= 2 ? 2 : 1; }
-
-template <class PF>
+template <class PF, int B>
 cudaError_t launch_col_adj_t(const AdjColWorld* worlds, int n, const AdjColArgs& args, const FastTables& t,
                              cudaStream_t s) {
-    constexpr int B = adj_col_batch(PF::n / PF::last());
     using K = ColK<PF, B>;
-    auto fn = col_adj_kernel<PF, B>;
-    const size_t smem = ColAdjK<PF, B>::smem();
-    if (smem > 227 * 1024 || K::T > 1024) return cudaErrorInvalidConfiguration;
-    cudaError_t e = prepare(fn, smem);
-    if (e != cudaSuccess) return e;
-    int per = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, K::T, smem);
-    fn<<<world_grid(per, (args.M + B - 1) / B, n), K::T, smem, s>>>(worlds, args, t.col_twf, t.col_twi);
-    return cudaGetLastError();
+    if constexpr (K::T > 1024) {
+        return cudaErrorInvalidConfiguration;
+    } else {
+        auto fn = col_adj_kernel<PF, B>;
+        const size_t smem = ColAdjK<PF, B>::smem();
+        if (smem > 227 * 1024) return cudaErrorInvalidConfiguration;
+        cudaError_t e = prepare(fn, smem);
+        if (e != cudaSuccess) return e;
+        int per = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, K::T, smem);
+        fn<<<world_grid(per, (args.M + B - 1) / B, n), K::T, smem, s>>>(worlds, args, t.col_twf, t.col_twi);
+        return cudaGetLastError();
+    }
 }
 
-template <class PI>
+template <class PI, int RB>
 cudaError_t launch_row_adj_t(const AdjRowWorld* worlds, int n, const AdjRowArgs& args, const float2* tw_r2c,
                              const FastTables& t, cudaStream_t s) {
-    constexpr int RB = adj_row_batch(PI::n / PI::last());
     using K = RowK<PI, RB>;
-    auto fn = row_adj_kernel<PI, RB>;
-    const size_t smem = K::smem();
-    if (smem > 227 * 1024) return cudaErrorInvalidConfiguration;
-    cudaError_t e = prepare(fn, smem);
-    if (e != cudaSuccess) return e;
-    int per = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, K::T, smem);
-    const int H = int(args.p.height);
-    fn<<<world_grid(per, (H + RB - 1) / RB, n), K::T, smem, s>>>(worlds, args, tw_r2c, t.row_twi, t.row_twf);
-    return cudaGetLastError();
+    if constexpr (K::T > 1024) {
+        return cudaErrorInvalidConfiguration;
+    } else {
+        auto fn = row_adj_kernel<PI, RB>;
+        const size_t smem = K::smem();
+        if (smem > 227 * 1024) return cudaErrorInvalidConfiguration;
+        cudaError_t e = prepare(fn, smem);
+        if (e != cudaSuccess) return e;
+        int per = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, K::T, smem);
+        const int H = int(args.p.height);
+        fn<<<world_grid(per, (H + RB - 1) / RB, n), K::T, smem, s>>>(worlds, args, tw_r2c, t.row_twi, t.row_twf);
+        return cudaGetLastError();
+    }
 }
 
-cudaError_t launch_col_adj(int H, const AdjColWorld* worlds, int n, const AdjColArgs& args, const FastTables& t,
-                           cudaStream_t s) {
+// batch: columns per CTA iteration (2, 4, 8); rows per CTA iteration (1, 2,
+// 4, 8). Candidates that do not fit a CTA return cudaErrorInvalidConfiguration.
+cudaError_t launch_col_adj(int H, int batch, const AdjColWorld* worlds, int n, const AdjColArgs& args,
+                           const FastTables& t, cudaStream_t s) {
     switch (H) {
-#define X(h, ...) \
-    case h: return launch_col_adj_t<__VA_ARGS__>(worlds, n, args, t, s);
+#define X(h, ...)                                                                         \
+    case h:                                                                               \
+        if (batch == 8) return launch_col_adj_t<__VA_ARGS__, 8>(worlds, n, args, t, s);   \
+        if (batch == 4) return launch_col_adj_t<__VA_ARGS__, 4>(worlds, n, args, t, s);   \
+        return launch_col_adj_t<__VA_ARGS__, 2>(worlds, n, args, t, s);
         LENIA_COL_PLANS(X)
 #undef X
     default: return cudaErrorNotSupported;
     }
 }
 
-cudaError_t launch_row_adj(int M, const AdjRowWorld* worlds, int n, const AdjRowArgs& args,
+cudaError_t launch_row_adj(int M, int batch, const AdjRowWorld* worlds, int n, const AdjRowArgs& args,
                            const float2* tw_r2c, const FastTables& t, cudaStream_t s) {
     switch (M) {
-#define X(m, ...) \
-    case m: return launch_row_adj_t<__VA_ARGS__>(worlds, n, args, tw_r2c, t, s);
+#define X(m, ...)                                                                                 \
+    case m:                                                                                       \
+        if (batch == 8) return launch_row_adj_t<__VA_ARGS__, 8>(worlds, n, args, tw_r2c, t, s);   \
+        if (batch == 4) return launch_row_adj_t<__VA_ARGS__, 4>(worlds, n, args, tw_r2c, t, s);   \
+        if (batch == 2) return launch_row_adj_t<__VA_ARGS__, 2>(worlds, n, args, tw_r2c, t, s);   \
+        return launch_row_adj_t<__VA_ARGS__, 1>(worlds, n, args, tw_r2c, t, s);
         LENIA_ROW_PLANS(X)
 #undef X
     default: return cudaErrorNotSupported;
@@ -542,7 +550,8 @@ struct lenia_adjoint {
     float* ckpt = nullptr;   // nck x nb x P: A_{jC} (last slot: A_T)
     float* seg = nullptr;    // C x nb x P: A_{s+i} inside a segment (i >= 1)
     float2* Sring = nullptr; // (C+1) x nb x SPX: row spectra of A_t
-    float2* Uring = nullptr; // C x nb x nk x SPX: potential spectra of step t
+    float2* Uspec = nullptr; // nb x nk x SPX: potential spectra (column -> row pass scratch)
+    float* Upx = nullptr;    // C x nb x nk x P: potentials of step t (kept by the row pass)
     float2* SQ = nullptr;    // nb x nk x SPX
     float2* SG = nullptr;    // nb x SPX
     float* g[2] = {nullptr, nullptr};  // nb x P: dL/dpre
@@ -556,13 +565,15 @@ struct lenia_adjoint {
     // Launch tables.
     lenia::SpectralWorld* d_r2c = nullptr;   // (nck-1) x nb
     lenia::SpectralWorld* d_fcol = nullptr;  // T x nb
-    lenia::SpectralWorld* d_frow = nullptr;  // T x nb
+    lenia::SpectralWorld* d_frow = nullptr;  // T x nb, recomputation (keeps every step's potentials)
+    lenia::SpectralWorld* d_ffwd = nullptr;  // T x nb, forward (keeps the last segment's potentials)
     lenia::AdjRowWorld* d_arow = nullptr;    // (T+1) x nb
     lenia::AdjColWorld* d_acol = nullptr;    // T x nb
     lenia::AdjRowArgs rargs{};
     lenia::AdjColArgs cargs{};
     lenia::StepParams params{};
-    int col_batch = 4, row_batch = 2;
+    int col_batch = 4, row_batch = 2;          // forward passes (autotuned)
+    int adj_col_batch = 4, adj_row_batch = 2;  // adjoint passes (autotuned)
     bool forward_done = false, last_segment_fresh = false;
 
     template <typename Tp>
@@ -594,7 +605,8 @@ struct lenia_adjoint {
         return seg + (size_t(t % C) * nb + b) * P;
     }
     float2* S_of(int t, int b) const { return Sring + (size_t(t % (C + 1)) * nb + b) * SPX; }
-    float2* U_of(int t, int b) const { return Uring + (size_t(t % C) * nb + b) * nk * SPX; }
+    float2* Uspec_of(int b) const { return Uspec + size_t(b) * nk * SPX; }
+    float* U_of(int t, int b) const { return Upx + (size_t(t % C) * nb + b) * nk * P; }
 
     int set_kernels(const lenia_kernel_def* kd, uint32_t n, float dt_new);
     int build_tables();
@@ -715,7 +727,9 @@ int lenia_adjoint::set_kernels(const lenia_kernel_def* kd, uint32_t n, float dt_
 // Every launch's world table (pointers per step and world).
 int lenia_adjoint::build_tables() {
     using namespace lenia;
-    std::vector<SpectralWorld> r2c(size_t(nck - 1) * nb), fcol(size_t(T) * nb), frow(size_t(T) * nb);
+    std::vector<SpectralWorld> r2c(size_t(nck - 1) * nb), fcol(size_t(T) * nb), frow(size_t(T) * nb),
+        ffwd(size_t(T) * nb);
+    const int last_segment = (nck - 2) * C;
     std::vector<AdjRowWorld> arow(size_t(T + 1) * nb);
     std::vector<AdjColWorld> acol(size_t(T) * nb);
     for (int b = 0; b < nb; ++b) {
@@ -732,20 +746,23 @@ int lenia_adjoint::build_tables() {
             SpectralWorld& c = fcol[size_t(t) * nb + b];
             c = SpectralWorld{};
             c.S = S_of(t, b);
-            c.U = U_of(t, b);
+            c.U = Uspec_of(b);
             c.khat = khat;
             c.M = M;
             c.nk = nk;
             c.p = params;
             SpectralWorld& r = frow[size_t(t) * nb + b];
             r = SpectralWorld{};
-            r.U = U_of(t, b);
+            r.U = Uspec_of(b);
+            r.U_px = U_of(t, b);
             r.A = slot(t, b);
             r.A_out = slot(t + 1, b);
             r.S_next = (t + 1 < T) ? S_of(t + 1, b) : nullptr;
             r.M = M;
             r.nk = nk;
             r.p = params;
+            ffwd[size_t(t) * nb + b] = r;
+            if (t < last_segment) ffwd[size_t(t) * nb + b].U_px = nullptr;
             AdjRowWorld& ar = arow[size_t(t) * nb + b];
             ar = AdjRowWorld{};
             ar.SG = (t == T - 1) ? nullptr : SG + size_t(b) * SPX;
@@ -773,6 +790,7 @@ int lenia_adjoint::build_tables() {
     up(d_r2c, r2c.data(), r2c.size() * sizeof(SpectralWorld));
     up(d_fcol, fcol.data(), fcol.size() * sizeof(SpectralWorld));
     up(d_frow, frow.data(), frow.size() * sizeof(SpectralWorld));
+    up(d_ffwd, ffwd.data(), ffwd.size() * sizeof(SpectralWorld));
     up(d_arow, arow.data(), arow.size() * sizeof(AdjRowWorld));
     up(d_acol, acol.data(), acol.size() * sizeof(AdjColWorld));
     if (e != cudaSuccess) return cuda_fail(e, "copy launch tables");
@@ -786,11 +804,13 @@ thread_local std::string g_adjoint_create_error;
 cudaStream_t pick_stream(lenia_adjoint* a, void* s) { return s ? static_cast<cudaStream_t>(s) : a->stream; }
 
 // The forward kernels over one step's world table.
-cudaError_t forward_step(lenia_adjoint* a, int t, cudaStream_t s) {
+// The forward kernels over one step's world tables (`recompute`: the tables
+// that keep the step's potentials).
+cudaError_t forward_step(lenia_adjoint* a, int t, bool recompute, cudaStream_t s) {
     using namespace lenia;
     cudaError_t e = launch_col_fast_worlds(a->H, a->M, a->ft, a->col_batch, a->d_fcol + size_t(t) * a->nb, a->nb, s);
-    if (e == cudaSuccess)
-        e = launch_row_fast_worlds(a->H, a->M, a->ft, a->tw_r2c, a->row_batch, a->d_frow + size_t(t) * a->nb, a->nb, s);
+    const SpectralWorld* rt = (recompute ? a->d_frow : a->d_ffwd) + size_t(t) * a->nb;
+    if (e == cudaSuccess) e = launch_row_fast_worlds(a->H, a->M, a->ft, a->tw_r2c, a->row_batch, rt, a->nb, s);
     a->launches += 2;
     return e;
 }
@@ -808,6 +828,8 @@ cudaError_t autotune(lenia_adjoint* a) {
     const cudaStream_t s = a->stream;
     cudaError_t e = cudaMemsetAsync(a->ckpt, 0, sizeof(float) * a->nb * a->P, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(a->Sring, 0, sizeof(float2) * a->nb * a->SPX, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(a->SG, 0, sizeof(float2) * a->nb * a->SPX, s);
+    for (int i = 0; i < 2 && e == cudaSuccess; ++i) e = cudaMemsetAsync(a->g[i], 0, sizeof(float) * a->nb * a->P, s);
     if (e != cudaSuccess) return e;
     cudaEvent_t t0, t1;
     cudaEventCreate(&t0);
@@ -853,6 +875,44 @@ cudaError_t autotune(lenia_adjoint* a) {
         if (ms < best) {
             best = ms;
             a->row_batch = rb;
+        }
+    }
+    // The adjoint passes, on step 0's tables (the row pass with the
+    // previous column pass's input, as in the steady state).
+    const int ta = a->T > 1 ? a->T - 2 : 0;
+    best = 1e30f;
+    for (int rb : {8, 4, 2, 1}) {
+        if (e != cudaSuccess) break;
+        float ms = 0.0f;
+        const cudaError_t r = timed([&] {
+            return lenia::launch_row_adj(a->M, rb, a->d_arow + size_t(ta) * a->nb, a->nb, a->rargs, a->tw_r2c, a->ft,
+                                         s);
+        }, &ms);
+        if (r == cudaErrorInvalidConfiguration) continue;
+        if (r != cudaSuccess) {
+            e = r;
+            break;
+        }
+        if (ms < best) {
+            best = ms;
+            a->adj_row_batch = rb;
+        }
+    }
+    best = 1e30f;
+    for (int cb : {8, 4, 2}) {
+        if (e != cudaSuccess) break;
+        float ms = 0.0f;
+        const cudaError_t r = timed([&] {
+            return lenia::launch_col_adj(a->H, cb, a->d_acol, a->nb, a->cargs, a->ft, s);
+        }, &ms);
+        if (r == cudaErrorInvalidConfiguration) continue;
+        if (r != cudaSuccess) {
+            e = r;
+            break;
+        }
+        if (ms < best) {
+            best = ms;
+            a->adj_col_batch = cb;
         }
     }
     cudaEventDestroy(t0);
@@ -912,7 +972,8 @@ int lenia_adjoint_create(const lenia_adjoint_config* cfg, lenia_adjoint** out) {
     if ((e = a->alloc(&a->ckpt, size_t(a->nck) * nb * a->P)) != cudaSuccess ||
         (e = a->alloc(&a->seg, size_t(a->C) * nb * a->P)) != cudaSuccess ||
         (e = a->alloc(&a->Sring, size_t(a->C + 1) * nb * a->SPX)) != cudaSuccess ||
-        (e = a->alloc(&a->Uring, size_t(a->C) * nb * nk * a->SPX)) != cudaSuccess ||
+        (e = a->alloc(&a->Uspec, nb * nk * a->SPX)) != cudaSuccess ||
+        (e = a->alloc(&a->Upx, size_t(a->C) * nb * nk * a->P)) != cudaSuccess ||
         (e = a->alloc(&a->SQ, nb * nk * a->SPX)) != cudaSuccess || (e = a->alloc(&a->SG, nb * a->SPX)) != cudaSuccess ||
         (e = a->alloc(&a->g[0], nb * a->P)) != cudaSuccess || (e = a->alloc(&a->g[1], nb * a->P)) != cudaSuccess ||
         (e = a->alloc(&a->gio, nb * a->P)) != cudaSuccess || (e = a->alloc(&a->acc, size_t(kAcc))) != cudaSuccess ||
@@ -921,6 +982,7 @@ int lenia_adjoint_create(const lenia_adjoint_config* cfg, lenia_adjoint** out) {
         (e = a->alloc(&a->d_r2c, size_t(a->nck - 1) * nb)) != cudaSuccess ||
         (e = a->alloc(&a->d_fcol, size_t(a->T) * nb)) != cudaSuccess ||
         (e = a->alloc(&a->d_frow, size_t(a->T) * nb)) != cudaSuccess ||
+        (e = a->alloc(&a->d_ffwd, size_t(a->T) * nb)) != cudaSuccess ||
         (e = a->alloc(&a->d_arow, size_t(a->T + 1) * nb)) != cudaSuccess ||
         (e = a->alloc(&a->d_acol, size_t(a->T) * nb)) != cudaSuccess)
         return bail(a->cuda_fail(e, "cudaMalloc"));
@@ -975,7 +1037,7 @@ int lenia_adjoint_forward(lenia_adjoint* a, const float* a0, float* a_final, voi
     const size_t n = size_t(a->nb) * a->P * sizeof(float);
     cudaError_t e = cudaMemcpyAsync(a->ckpt, a0, n, cudaMemcpyDeviceToDevice, s);
     if (e == cudaSuccess) e = row_spectrum(a, 0, s);
-    for (int t = 0; t < a->T && e == cudaSuccess; ++t) e = forward_step(a, t, s);
+    for (int t = 0; t < a->T && e == cudaSuccess; ++t) e = forward_step(a, t, false, s);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(a_final, a->slot(a->T, 0), n, cudaMemcpyDeviceToDevice, s);
     if (e != cudaSuccess) return a->cuda_fail(e, "forward");
@@ -997,16 +1059,19 @@ int lenia_adjoint_backward(lenia_adjoint* a, const float* g_final, float* g_init
         const int s0 = j * a->C, e0 = std::min(s0 + a->C, a->T);
         if (!(j == a->nck - 2 && a->last_segment_fresh)) {
             e = row_spectrum(a, j, s);
-            for (int t = s0; t < e0 && e == cudaSuccess; ++t) e = forward_step(a, t, s);
+            for (int t = s0; t < e0 && e == cudaSuccess; ++t) e = forward_step(a, t, true, s);
         }
         for (int t = e0 - 1; t >= s0 && e == cudaSuccess; --t) {
-            e = launch_row_adj(a->M, a->d_arow + size_t(t) * a->nb, a->nb, a->rargs, a->tw_r2c, a->ft, s);
-            if (e == cudaSuccess) e = launch_col_adj(a->H, a->d_acol + size_t(t) * a->nb, a->nb, a->cargs, a->ft, s);
+            e = launch_row_adj(a->M, a->adj_row_batch, a->d_arow + size_t(t) * a->nb, a->nb, a->rargs, a->tw_r2c,
+                               a->ft, s);
+            if (e == cudaSuccess)
+                e = launch_col_adj(a->H, a->adj_col_batch, a->d_acol + size_t(t) * a->nb, a->nb, a->cargs, a->ft, s);
             a->launches += 2;
         }
     }
     if (e == cudaSuccess) {
-        e = launch_row_adj(a->M, a->d_arow + size_t(a->T) * a->nb, a->nb, a->rargs, a->tw_r2c, a->ft, s);
+        e = launch_row_adj(a->M, a->adj_row_batch, a->d_arow + size_t(a->T) * a->nb, a->nb, a->rargs, a->tw_r2c,
+                           a->ft, s);
         a->launches += 1;
     }
     if (e == cudaSuccess) e = cudaMemcpyAsync(g_initial, a->gio, n, cudaMemcpyDeviceToDevice, s);

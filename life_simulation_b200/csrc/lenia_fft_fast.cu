@@ -243,6 +243,11 @@ __global__ void __launch_bounds__(RowK<PI, RB>::T, (512 / RowK<PI, RB>::T > 1 ? 
                 IL::template twiddle<true>(z, jj[it], twi);
                 Dft<RC, true>::run(z);
                 const uint32_t gy = uint32_t(y0 + bi[it]);
+                if (sw.U_px) {  // keep the potentials (the adjoint's recomputation)
+                    float* up = sw.U_px + (size_t(kk) * H + gy) * W;
+#pragma unroll
+                    for (int t = 0; t < RC; ++t) *reinterpret_cast<float2*>(up + 2 * (jj[it] + t * NRC)) = z[t];
+                }
 #pragma unroll
                 for (int t = 0; t < RC; ++t) {
                     const uint32_t x0 = uint32_t(2 * (jj[it] + t * NRC));

@@ -105,6 +105,7 @@ struct SpectralWorld {
     const float* A;      // state in
     float* A_out;        // state out
     float2* S_next;      // row spectrum of A_out, or null
+    float* U_px;         // row pass: nk potential planes (H x W) to keep, or null
     int M;               // columns of the half spectrum (W/2)
     int nk;              // kernels (0: row pass computes only S_next of A)
     StepParams p;

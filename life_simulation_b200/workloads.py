@@ -9,10 +9,15 @@ from a seed by SplitMix64 (the algorithm of LifeCore/Math/Random.h:11-31,
   in the central 64x64 square (seed 1), zeros elsewhere.
 * ``adjoint_512`` (the gradient form): 32 worlds of 512x512, two kernels
   R=16, peaks [1] and [0.5, 1], mu {0.15, 0.25}, sigma {0.015, 0.03},
-  weights {0.5, 0.5}, dt 0.1, growth mode 0, exponential core, T=64 steps
-  with checkpoints every 8; world b starts from uniform[0,1) over the whole
-  field (SplitMix64 seed 4000 + b) and its target is the T-step state from
-  seed 5000 + b; loss = mean squared error over every world and pixel.
+  weights {0.5, 0.5}, dt 0.1, growth mode 1 (asymptotic: A += dt (G - A)),
+  exponential core, T=64 steps with checkpoints every 8; world b starts from
+  uniform[0,1) over the whole field (SplitMix64 seed 4000 + b) and its target
+  is the T-step state from seed 5000 + b; loss = mean squared error over
+  every world and pixel. Under growth mode 0 these kernels take every
+  seeded start (whole field, central square or patches, any amplitude)
+  to the all-zero field within ~25 steps, where the clip mask makes the
+  T=64 gradient identically zero; growth mode 1 keeps every pixel strictly
+  inside (0, 1), so every term of the backward pass is live.
 * ``fft3_1080p`` / ``fft3_1024x512``: three kernels of radius 24, peaks
   [1], [0.5, 1], [1, 0.667, 0.333], mu {0.156, 0.193, 0.342}, sigma
   {0.0118, 0.049, 0.0891}, weights {0.5, 0.3, 0.2}, dt 0.1, growth mode 0,
@@ -91,7 +96,7 @@ ADJOINT_KERNELS = [
     {"mu": 0.25, "sigma": 0.03, "weight": 0.5, "betas": [0.5, 1.0]},
 ]
 ADJOINT_512 = {"width": 512, "height": 512, "batch": 32, "radius": 16, "steps": 64,
-               "checkpoint_every": 8, "dt": 0.1, "growth_mode": 0}
+               "checkpoint_every": 8, "dt": 0.1, "growth_mode": 1}
 
 
 def adjoint_fields(seed_base: int, batch: int = 32, w: int = 512, h: int = 512) -> np.ndarray:

@@ -196,6 +196,37 @@ def test_full_size_batch_512():
         assert abs(gp1[i] - v) <= 2e-3 * abs(v) + 1e-6 * np.abs(ref).max(), (i, gp1[i], v)
 
 
+def test_benchmark_workload_against_fp64_oracle():
+    """The benchmarked adjoint workload itself (growth mode 1, seeded
+    uniform[0,1) fields, targets from a forward run of other seeds, T=64,
+    checkpoints every 8) for two of its 32 worlds: live, non-zero gradients
+    that agree with the FP64 oracle's adjoint."""
+    from life_simulation_b200 import workloads as wl
+    c = wl.ADJOINT_512
+    w, h, steps = c["width"], c["height"], c["steps"]
+    eng = lb.LeniaAdjoint(w, h, 2, wl.ADJOINT_KERNELS, c["radius"], steps, c["checkpoint_every"], c["dt"],
+                          c["growth_mode"], lb.CORE_EXP)
+    a0 = wl.adjoint_fields(4000, 2, w, h).astype(np.float32)
+    s = torch.cuda.current_stream().cuda_stream
+    t0 = torch.from_numpy(wl.adjoint_fields(5000, 2, w, h).astype(np.float32)).cuda()
+    tgt = torch.empty_like(t0)
+    eng.forward(t0.data_ptr(), tgt.data_ptr(), s)
+    target = tgt.cpu().numpy()
+    aT, ga0, gp = run_engine(eng, a0, target)
+    eng.close()
+    assert ((aT > 0) & (aT < 1)).all()
+    p = oracle_params(wl.ADJOINT_KERNELS, c["radius"], c["dt"], c["growth_mode"], lb.CORE_EXP)
+    states = O.forward(a0[0].astype(np.float64), p, steps)
+    assert np.abs(aT[0] - states[-1]).max() < 1e-4
+    _, g = O.loss_and_grads(a0.astype(np.float64), target.astype(np.float64), p, steps)
+    assert np.abs(g.field).max() > 0.0
+    assert np.abs(ga0 - g.field).max() <= 2e-3 * np.abs(g.field).max()
+    ref = oracle_vector(g, p)
+    assert np.abs(ref).max() > 0.0
+    for i, v in enumerate(ref):
+        assert abs(gp[i] - v) <= 2e-3 * abs(v) + 1e-6 * np.abs(ref).max(), (i, gp[i], v)
+
+
 def test_invalid_configs_are_rejected():
     with pytest.raises(lb.LeniaError, match="no compile-time FFT plan"):
         lb.LeniaAdjoint(100, 100, 1, KERNELS, 8, 4)
