@@ -10,14 +10,19 @@ pixels x steps; ``value`` is whole-job Mpixel-steps/s.
   the launching stream, with a 256 MiB write between steps to flush the
   126 MB L2 (outside the events); time = sum of the step intervals, max over
   ranks. Under torchrun every rank steps its own world (replicas, no
-  collective on the data path; weak scaling).
+  collective on the data path; weak scaling). Before the warm-up the launch
+  shapes of the two passes are chosen under these same conditions
+  (lenia_set_tuning; --keep-tuning keeps the setup autotuner's).
 * e2e: the same metric through the C ABI with host buffers: per step
   lenia_upload (pinned host -> device), lenia_step, lenia_download (device ->
   pinned host), timed by CUDA events on the context stream.
 * roofline: the dominant kernel's algorithmic bytes per launch (HBM-bound
   figures of the spectral path, per pixel: column pass 4 + 2K + 4K, row
-  growth pass 4K + 4 + 4 + 4) over its mean event-timed launch duration,
-  against the measured copy bandwidth in MEASURED_PEAKS.json.
+  growth pass 4K + 4 + 4 + 4) over its mean launch duration, timed by CUDA
+  events around every launch over further flushed steps (events between
+  launches serialise them, so the durations are upper bounds; the value
+  region has none), against the measured copy bandwidth in
+  MEASURED_PEAKS.json.
 * cpu_baseline: the reference's own Lenia module and kernels compiled for
   the CPU (oracle/_ref), on a bounded row band of the same workload.
 * adjoint: the gradient form on 32 worlds of 512x512 (K=2, R=16, growth
@@ -71,6 +76,9 @@ def parse_args():
                          "on FP32 CUDA cores vs split-precision tensor cores")
     ap.add_argument("--adjoint-reps", type=int, default=5)
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--keep-tuning", action="store_true",
+                    help="keep the setup autotuner's launch shapes instead of choosing them under the "
+                         "bench's own conditions (flushed L2) before the timed region")
     ap.add_argument("--plain-steps", type=int, default=10)
     return ap.parse_args()
 
@@ -271,6 +279,40 @@ def run_b200(args):
             torch.distributed.barrier()
             torch.cuda.synchronize()
 
+    def run_steps(n, first):
+        """n steps, the L2 flushed before each; per-step CUDA-event times (ms)
+        on the bench stream."""
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(n)]
+        for i in range(n):
+            flush.zero_()
+            fp.frame_index = fp.audio_frame = first + i
+            evs[i][0].record(stream)
+            m.step(fp, 1, sh)
+            evs[i][1].record(stream)
+        barrier()
+        return [a.elapsed_time(b) for a, b in evs]
+
+    # Launch shapes (columns / rows per CTA of the two passes) chosen under
+    # this run's own conditions -- the L2 flushed before every step -- by
+    # timing each supported shape outside the timed region; then the state
+    # is reset so the timed steps start from the same field as without it.
+    shape, chosen_by = m.tuning(), "setup autotuner"
+    if shape != (0, 0) and not args.keep_tuning:
+        best = None
+        for c in (8, 4, 2):
+            for r in (4, 2, 1, 4 | lb.ROWS_PIPELINED, 2 | lb.ROWS_PIPELINED, 1 | lb.ROWS_PIPELINED):
+                try:
+                    m.set_tuning(c, r)
+                except lb.LeniaError:
+                    continue  # over the thread or shared-memory limit at this size
+                run_steps(3, 0)
+                t = statistics.median(run_steps(30, 0))
+                if best is None or t < best[0]:
+                    best = (t, (c, r))
+        shape, chosen_by = best[1], "bench: median of 30 flushed steps per shape"
+        m.set_tuning(*shape)
+        m.reset(2 + rank)
+        m.upload(init)
     for i in range(max(3, args.warmup)):
         fp.frame_index = fp.audio_frame = i
         m.step(fp, 1, sh)
@@ -278,20 +320,20 @@ def run_b200(args):
     clocks = ClockSampler(local)
     clocks.start()
     time.sleep(0.3)
+    m.profile(False)  # resets the launch counter; no per-launch events
+    step_ms = run_steps(args.steps, args.warmup)
+    launches = m.profile_read()["launches"]
+    cl = clocks.stop()
+    total_ms = float(sum(step_ms))
+    # Per-kernel durations for the roofline: the same steps again with CUDA
+    # events around every launch (events between the two passes serialise
+    # them, so these durations are an upper bound; the step value above is
+    # timed without them).
+    prof_steps = min(args.steps, 100)
     m.profile(True)
-    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    for i in range(args.steps):
-        flush.zero_()
-        fp.frame_index = fp.audio_frame = args.warmup + i
-        evs[i][0].record(stream)
-        m.step(fp, 1, sh)
-        evs[i][1].record(stream)
-    barrier()
+    run_steps(prof_steps, args.warmup + args.steps)
     prof = m.profile_read()
     m.profile(False)
-    cl = clocks.stop()
-    step_ms = [a.elapsed_time(b) for a, b in evs]
-    total_ms = float(sum(step_ms))
     if world > 1:
         t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
@@ -335,11 +377,15 @@ def run_b200(args):
     step_bytes = (20 + 10 * K) * w * h  # canonical three-sweep bytes per pixel-step
     mean_step_ms = total_ms / args.steps
     line = base_line(args, world, args.steps, args.warmup, w, h, params)
+    if shape != (0, 0):
+        line["config"]["launch_shape"] = {"cols_per_cta": shape[0], "rows_per_cta": shape[1] & 0xFF,
+                                          "rows_pipelined": bool(shape[1] & lb.ROWS_PIPELINED),
+                                          "chosen_by": chosen_by}
     line.update({
         "value": value, "ms_per_step": mean_step_ms,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(w * h * 4),
                 "d2h_bytes_per_step": int(w * h * 4), "steps": e2e_steps},
-        "gpu_launches": int(prof["launches"]),
+        "gpu_launches": int(launches),
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                      "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": NCU_TRAFFIC_BYTES.get(dom),
@@ -347,7 +393,8 @@ def run_b200(args):
                      "launch_ms": launch_ms,
                      "step": {"bytes": step_bytes, "achieved": step_bytes / (mean_step_ms / 1e3) / 1e9,
                               "frac": step_bytes / (mean_step_ms / 1e3) / 1e9 / peak}},
-        "phases_ms_per_step": {k: v["ms"] / args.steps for k, v in phases.items()},
+        "phases_ms_per_step": {k: v["ms"] / prof_steps for k, v in phases.items()},
+        "kernel_timing": f"per-launch CUDA events over {prof_steps} further flushed steps",
         "clocks": cl,
     })
     if rank == 0 and world == 1 and not args.no_adjoint:

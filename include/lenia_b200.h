@@ -229,6 +229,17 @@ typedef struct lenia_profile_data {
 } lenia_profile_data;
 int lenia_profile(lenia_ctx* ctx, int enable);
 int lenia_profile_read(lenia_ctx* ctx, lenia_profile_data* out);
+/* Launch shapes of the spectral passes (extension; the reference has no
+ * counterpart): columns per CTA of the column pass (8, 4 or 2) and rows per
+ * CTA of the inverse row pass (4, 2 or 1, | LENIA_ROWS_PIPELINED for the
+ * software-pipelined variant), as the setup autotuner picked them; 0, 0 on
+ * the direct path and on the runtime-plan spectral path. lenia_set_tuning
+ * replaces them until the next setup (reproducible timings, or a choice
+ * made under the caller's own conditions); a shape the field size cannot
+ * launch, or a context without these passes, is LENIA_ERR_INVALID_ARG. */
+#define LENIA_ROWS_PIPELINED 0x100
+int lenia_get_tuning(lenia_ctx* ctx, int* cols_per_cta, int* rows_per_cta);
+int lenia_set_tuning(lenia_ctx* ctx, int cols_per_cta, int rows_per_cta);
 /* ---- Colour map (the module's output layer) ----
  * The field as an RGBA16F image through the module's cosine palette
  * (Shaders/Render/ColorMap.metal: t = clamp(v * input_scale + input_bias,

@@ -32,6 +32,7 @@ LENIA_WARN_FALLBACK = 1
 CONV_DIRECT, CONV_FFT, CONV_DIRECT_MULTI = 0, 1, 2
 CORE_GAUSS_SHELL, CORE_EXP = 0, 1
 FFT_FP32, FFT_BF16X3, FFT_FP16X3 = 0, 1, 2
+ROWS_PIPELINED = 0x100  # rows-per-CTA flag of the software-pipelined row pass
 INIT_NOISE, INIT_STAMP = 0, 1
 
 
@@ -90,7 +91,7 @@ EXPORTS = (
     "lenia_resolve_frame_params", "lenia_encode", "lenia_step", "lenia_sync",
     "lenia_field_size", "lenia_upload", "lenia_download", "lenia_upload_device",
     "lenia_download_device", "lenia_field_device_ptr", "lenia_get_info",
-    "lenia_get_stream", "lenia_profile", "lenia_profile_read",
+    "lenia_get_stream", "lenia_profile", "lenia_profile_read", "lenia_get_tuning", "lenia_set_tuning",
     "lenia_last_message", "lenia_status_string",
     "lenia_fft_step_noalloc", "lenia_noalloc_last_message",
     "lenia_batch_create", "lenia_batch_destroy", "lenia_batch_upload", "lenia_batch_download",
@@ -199,6 +200,8 @@ def load_library(path: str = LIB_PATH):
     L.lenia_get_stream.argtypes = [P, pp]
     L.lenia_profile.argtypes = [P, i32]
     L.lenia_profile_read.argtypes = [P, ctypes.POINTER(ProfileData)]
+    L.lenia_get_tuning.argtypes = [P, ctypes.POINTER(i32), ctypes.POINTER(i32)]
+    L.lenia_set_tuning.argtypes = [P, i32, i32]
     L.lenia_last_message.argtypes = [P]
     L.lenia_last_message.restype = ctypes.c_char_p
     L.lenia_status_string.argtypes = [i32]
@@ -458,6 +461,17 @@ class LeniaModule:
         for i, name in enumerate(PHASES):
             out[name] = {"count": int(d.count[i]), "ms": float(d.ms[i])}
         return out
+
+    def tuning(self) -> tuple:
+        """(columns per CTA, rows per CTA) of the spectral passes as tuned
+        at setup (rows may carry ROWS_PIPELINED); (0, 0) without them."""
+        c, r = ctypes.c_int32(), ctypes.c_int32()
+        self._check(self._L.lenia_get_tuning(self._h, ctypes.byref(c), ctypes.byref(r)))
+        return c.value, r.value
+
+    def set_tuning(self, cols_per_cta: int, rows_per_cta: int) -> None:
+        """Replaces the tuned launch shapes until the next setup."""
+        self._check(self._L.lenia_set_tuning(self._h, int(cols_per_cta), int(rows_per_cta)))
 
     def info(self) -> dict:
         i = Info()

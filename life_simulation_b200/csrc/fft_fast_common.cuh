@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 
 #include "fft_ct.cuh"
 #include "lenia_kernels.h"
@@ -228,6 +229,46 @@ cudaError_t prepare(F fn, size_t smem) {
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+}
+
+// Programmatic dependent launch. A kernel launched by `launch_chained` may
+// start while the kernel before it in the stream is still running: it does
+// its data-independent prologue (twiddle tables into shared memory), then
+// `grid_dependency_wait` blocks until that kernel has completed and its
+// writes are visible. `allow_dependents`, called when a CTA starts its last
+// work item, lets the next chained kernel launch once every CTA of this one
+// has called it (or exited): the next kernel's CTAs then do their prologue
+// while this kernel's last items finish. Every CTA of a chained kernel
+// waits before it touches data, so kernel completion stays transitive along
+// the stream. Both instructions are no-ops in a kernel launched without the
+// attribute.
+__device__ __forceinline__ void grid_dependency_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+__device__ __forceinline__ void allow_dependents() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
+
+// LENIA_CHAINED_LAUNCH=0 in the environment turns the attribute off (plain
+// stream order), e.g. for tools that serialise launches anyway.
+inline bool chained_launch_enabled() {
+    static const bool on = [] {
+        const char* v = std::getenv("LENIA_CHAINED_LAUNCH");
+        return !(v && v[0] == '0' && v[1] == '\0');
+    }();
+    return on;
+}
+
+template <typename... KArgs, typename... Args>
+cudaError_t launch_chained(void (*fn)(KArgs...), dim3 grid, int threads, size_t smem, cudaStream_t s,
+                           Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = dim3(unsigned(threads));
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = chained_launch_enabled() ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, fn, args...);
 }
 
 // Persistent grid over n worlds: grid.y = world, grid.x = CTAs per world

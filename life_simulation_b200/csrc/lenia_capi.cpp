@@ -353,6 +353,19 @@ int lenia_profile_read(lenia_ctx* c, lenia_profile_data* out) {
     return guarded(c, [&] { return c->module.readProfile(out); });
 }
 
+static_assert(LENIA_ROWS_PIPELINED == lenia::kRowPipelined, "pipelined row flag");
+
+int lenia_get_tuning(lenia_ctx* c, int* cols, int* rows) {
+    if (!c || !cols || !rows) return LENIA_ERR_INVALID_ARG;
+    c->module.tuning(cols, rows);
+    return LENIA_OK;
+}
+
+int lenia_set_tuning(lenia_ctx* c, int cols, int rows) {
+    if (!c) return LENIA_ERR_INVALID_ARG;
+    return guarded(c, [&] { return set_msg(c, c->module.setTuning(cols, rows)); });
+}
+
 // ---------------------------------------------------------- colour map
 
 static_assert(sizeof(lenia_colormap) == sizeof(lenia::ColorMapParams), "colour map layout");

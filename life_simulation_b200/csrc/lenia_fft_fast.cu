@@ -61,7 +61,6 @@ __global__ void __launch_bounds__(ColK<PF, B>::T)
     constexpr int H = K::H, T = K::T, PITCH = K::PITCH, RL = K::RL, NRL = K::NRL, Hh = K::Hh;
     extern __shared__ __align__(16) float2 sm[];
     __shared__ SpectralWorld sw;  // this CTA's world
-    if (threadIdx.x == 0) sw = worlds ? worlds[blockIdx.y] : w0;
     float2* twf = sm;
     float2* twi = twf + PF::tw_size();
     float2* ba = twi + PI::tw_size();
@@ -69,12 +68,16 @@ __global__ void __launch_bounds__(ColK<PF, B>::T)
     float2* c0 = bb + B * PITCH;
     copy_table(twf, twf_g, PF::tw_size());
     copy_table(twi, twi_g, PI::tw_size());
+    grid_dependency_wait();
+    if (threadIdx.x == 0) sw = worlds ? worlds[blockIdx.y] : w0;
     __syncthreads();
     const float2* __restrict__ S = sw.S;
     float2* __restrict__ U = sw.U;
     const float* __restrict__ khat = sw.khat;
     const int M = sw.M, nk = sw.nk;
+    if (int(blockIdx.x) * B >= M) allow_dependents();
     for (int k0 = blockIdx.x * B; k0 < M; k0 += gridDim.x * B) {
+        if (k0 + int(gridDim.x) * B >= M) allow_dependents();  // this CTA's last group
         const int cols = min(B, M - k0);
         // Element (b, ky) of this group in the blocked layout.
         const size_t gbase = size_t(k0 / KB) * H * KB + (k0 % KB);
@@ -166,7 +169,6 @@ __global__ void __launch_bounds__(RowK<PI, RB>::T, (512 / RowK<PI, RB>::T > 1 ? 
     constexpr int M = K::M, W = 2 * M, T = K::T, PITCH = K::PITCH, RC = K::RC, NRC = K::NRC;
     extern __shared__ __align__(16) float2 sm[];
     __shared__ SpectralWorld sw;  // this CTA's world
-    if (threadIdx.x == 0) sw = worlds ? worlds[blockIdx.y] : w0;
     float2* twr = sm;
     float2* twi = twr + (M + 1);
     float2* twf = twi + PI::tw_size();
@@ -176,6 +178,8 @@ __global__ void __launch_bounds__(RowK<PI, RB>::T, (512 / RowK<PI, RB>::T > 1 ? 
     copy_table(twr, twr_g, M + 1);
     copy_table(twi, twi_g, PI::tw_size());
     copy_table(twf, twf_g, PF::tw_size());
+    grid_dependency_wait();
+    if (threadIdx.x == 0) sw = worlds ? worlds[blockIdx.y] : w0;
     __syncthreads();
     const float2* __restrict__ U = sw.U;
     const float* __restrict__ A = sw.A;
@@ -199,7 +203,9 @@ __global__ void __launch_bounds__(RowK<PI, RB>::T, (512 / RowK<PI, RB>::T > 1 ? 
         stage(stg[0], int(blockIdx.x) * RB, 0);
         cp_async_commit();
     }
+    if (int(blockIdx.x) * RB >= H) allow_dependents();
     for (int y0 = blockIdx.x * RB; y0 < H; y0 += gridDim.x * RB) {
+        if (y0 + int(gridDim.x) * RB >= H) allow_dependents();  // this CTA's last row group
         const int rows = min(RB, H - y0);
         int jj[K::ITL], bi[K::ITL];
         bool ok[K::ITL];
@@ -343,8 +349,7 @@ cudaError_t launch_col_t(const SpectralWorld& w0, const SpectralWorld* worlds, i
     if (e != cudaSuccess) return e;
     int per = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, K::T, smem);
-    fn<<<world_grid(per, (M + B - 1) / B, n), K::T, smem, s>>>(w0, worlds, t.col_twf, t.col_twi);
-    return cudaGetLastError();
+    return launch_chained(fn, world_grid(per, (M + B - 1) / B, n), K::T, smem, s, w0, worlds, t.col_twf, t.col_twi);
 }
 
 template <class PI, int RB, bool PIPE>
@@ -358,8 +363,8 @@ cudaError_t launch_row_t(const SpectralWorld& w0, const SpectralWorld* worlds, i
     if (e != cudaSuccess) return e;
     int per = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, K::T, smem);
-    fn<<<world_grid(per, (H + RB - 1) / RB, n), K::T, smem, s>>>(w0, worlds, tw_r2c, t.row_twi, t.row_twf);
-    return cudaGetLastError();
+    return launch_chained(fn, world_grid(per, (H + RB - 1) / RB, n), K::T, smem, s, w0, worlds, tw_r2c, t.row_twi,
+                          t.row_twf);
 }
 
 }  // namespace
@@ -451,7 +456,52 @@ cudaError_t row_dispatch(int H, int M, int batch, const SpectralWorld& w0, const
     }
 }
 
+template <class PF, int B>
+bool col_shape_ok() {
+    using K = ColK<PF, B>;
+    return K::T <= 1024 && K::smem() <= 227 * 1024;
+}
+
+template <class PI, int RB, bool PIPE>
+bool row_shape_ok() {
+    using K = RowK<PI, RB>;
+    return K::T <= 1024 && K::smem(PIPE ? 3 : 2) <= 227 * 1024;
+}
+
 }  // namespace
+
+bool fast_shapes_supported(int H, int M, int col_batch, int row_batch) {
+    bool col = false, row = false;
+    switch (H) {
+#define X(h, ...)                                                        \
+    case h:                                                              \
+        col = col_batch == 8   ? col_shape_ok<__VA_ARGS__, 8>()          \
+              : col_batch == 4 ? col_shape_ok<__VA_ARGS__, 4>()          \
+              : col_batch == 2 ? col_shape_ok<__VA_ARGS__, 2>() : false; \
+        break;
+        LENIA_COL_PLANS(X)
+#undef X
+    default: break;
+    }
+    const int rb = row_batch & ~kRowPipelined;
+    const bool pipe = (row_batch & kRowPipelined) != 0;
+    if ((row_batch & ~(kRowPipelined | 7)) != 0) return false;
+    switch (M) {
+#define X(m, ...)                                                                                      \
+    case m:                                                                                            \
+        row = pipe ? (rb == 4   ? row_shape_ok<__VA_ARGS__, 4, true>()                                 \
+                      : rb == 2 ? row_shape_ok<__VA_ARGS__, 2, true>()                                 \
+                      : rb == 1 ? row_shape_ok<__VA_ARGS__, 1, true>() : false)                        \
+                   : (rb == 4   ? row_shape_ok<__VA_ARGS__, 4, false>()                                \
+                      : rb == 2 ? row_shape_ok<__VA_ARGS__, 2, false>()                                \
+                      : rb == 1 ? row_shape_ok<__VA_ARGS__, 1, false>() : false);                      \
+        break;
+        LENIA_ROW_PLANS(X)
+#undef X
+    default: break;
+    }
+    return col && row;
+}
 
 cudaError_t launch_col_fast(const FftGeometry& g, const FastTables& t, int batch, const float2* S,
                             float2* U, cudaStream_t s) {

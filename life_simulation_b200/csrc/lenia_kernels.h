@@ -127,6 +127,10 @@ bool fast_twiddle_tables(int H, int M, std::vector<float2> (&out)[4]);
 constexpr int kRowPipelined = 0x100;
 // The row-batch candidates an autotuner times.
 constexpr int kRowCandidates[6] = {4, 2, 1, 4 | kRowPipelined, 2 | kRowPipelined, 1 | kRowPipelined};
+// Whether columns per CTA `col_batch` (8/4/2) and rows per CTA `row_batch`
+// (4/2/1, optionally | kRowPipelined) launch for an H x 2M field on the
+// compile-time-plan passes (thread count and shared memory within limits).
+bool fast_shapes_supported(int H, int M, int col_batch, int row_batch);
 cudaError_t launch_col_fast(const FftGeometry& g, const FastTables& t, int batch, const float2* S,
                             float2* U, cudaStream_t s);
 cudaError_t launch_row_fast(const FftGeometry& g, const FastTables& t, int batch, const float2* U,

@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <fstream>
 #include <sstream>
@@ -887,15 +888,30 @@ int LeniaModule::autotuneSpectral() {
     };
     // A candidate must beat the current choice by 3 % to replace it (the
     // timings run with warm caches; larger batches coalesce better cold).
+    // LENIA_AUTOTUNE_LOG=1 prints every candidate's time to stderr.
+    const char* log_env = std::getenv("LENIA_AUTOTUNE_LOG");
+    const bool log = log_env && *log_env && *log_env != '0';
     float best_col = 1e30f, best_row = 1e30f;
     for (int c : {8, 4, 2}) {
         const float t = time_it([&] { return launch_col_fast(fgeo_, fast_, c, d_S_, d_U_, stream_); });
+        if (log) std::fprintf(stderr, "lenia autotune %ux%u column cols/CTA %d: %.4f ms\n", w_, h_, c, t);
         if (t < 0.97f * best_col) { best_col = t; col_batch_ = c; }
     }
+    // Row candidates are timed as they run in a step: three column + row
+    // pairs back to back (the row pass follows the column pass it reads).
     for (int c : kRowCandidates) {
         const float t = time_it([&] {
-            return launch_row_fast(fgeo_, fast_, c, d_U_, field_[0], field_[1], d_S_, p, fgeo_.nk, stream_);
+            cudaError_t e = cudaSuccess;
+            for (int i = 0; i < 3 && e == cudaSuccess; ++i) {
+                e = launch_col_fast(fgeo_, fast_, col_batch_, d_S_, d_U_, stream_);
+                if (e == cudaSuccess)
+                    e = launch_row_fast(fgeo_, fast_, c, d_U_, field_[0], field_[1], d_S_, p, fgeo_.nk, stream_);
+            }
+            return e;
         });
+        if (log)
+            std::fprintf(stderr, "lenia autotune %ux%u 3 steps with rows/CTA %d%s: %.4f ms\n", w_, h_, c & ~kRowPipelined,
+                         (c & kRowPipelined) ? " pipelined" : "", t);
         if (t < 0.97f * best_row) { best_row = t; row_batch_ = c; }
     }
     if (tc_precision_ != LENIA_FFT_FP32) {
@@ -912,6 +928,24 @@ int LeniaModule::autotuneSpectral() {
     event_pool_.push_back(b);
     cudaMemsetAsync(field_[0], 0, sizeof(float) * w_ * h_, stream_);
     cudaMemsetAsync(field_[1], 0, sizeof(float) * w_ * h_, stream_);
+    return LENIA_OK;
+}
+
+void LeniaModule::tuning(int* cols, int* rows) const {
+    const bool on = fast_col_ && fast_row_;
+    *cols = on ? col_batch_ : 0;
+    *rows = on ? row_batch_ : 0;
+}
+
+int LeniaModule::setTuning(int cols, int rows) {
+    if (!(fast_col_ && fast_row_))
+        return fail(LENIA_ERR_INVALID_ARG, "launch shapes apply to the compile-time-plan spectral passes only");
+    if (!fast_shapes_supported(int(h_), int(w_ / 2), cols, rows))
+        return fail(LENIA_ERR_INVALID_ARG, "unsupported launch shape: " + std::to_string(cols) + " columns, " +
+                                               std::to_string(rows) + " rows per CTA for " + std::to_string(w_) +
+                                               "x" + std::to_string(h_));
+    col_batch_ = cols;
+    row_batch_ = rows;
     return LENIA_OK;
 }
 

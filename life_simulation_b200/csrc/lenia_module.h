@@ -121,6 +121,11 @@ public:
     void setMessage(std::string m) { message_ = std::move(m); }
     cudaStream_t stream() const { return stream_; }
 
+    // Launch shapes of the compile-time-plan spectral passes (columns and
+    // rows per CTA; 0, 0 when the context does not use them).
+    void tuning(int* cols, int* rows) const;
+    int setTuning(int cols, int rows);
+
     // Per-launch event timing (GPUTimer's role, LifeCore/Metal/GPUTimer.h).
     void setProfiling(bool on);
     int readProfile(lenia_profile_data* out);

@@ -204,6 +204,46 @@ def test_determinism_same_seed_same_bits():
     np.testing.assert_array_equal(runs[0], runs[1])
 
 
+@pytest.mark.parametrize("w,h", [(1920, 1080), (512, 512)])
+def test_every_launch_shape_gives_the_same_bits(w, h):
+    """Rows and columns are transformed independently with one plan, so the
+    field must not depend on the rows/columns per CTA the autotuner picks."""
+    p = wl.fft3_params(w, h)
+    p["noiseAmount"] = 0.1
+    init = wl.patches(w, h, 8, 64, seed=6)
+    m = lb.LeniaModule(p, w, h)
+    cols, rows = m.tuning()
+    assert cols in (8, 4, 2) and rows & ~lb.ROWS_PIPELINED in (4, 2, 1)
+    ref = None
+    shapes = [(c, r | f) for c in (8, 4, 2) for r in (4, 2, 1) for f in (0, lb.ROWS_PIPELINED)]
+    ran = 0
+    for c, r in shapes:
+        try:
+            m.set_tuning(c, r)
+        except lb.LeniaError:
+            continue  # a shape over the thread or shared-memory limit
+        assert m.tuning() == (c, r)
+        m.reset(1)
+        m.upload(init)
+        for f in range(3):
+            m.encode(f, 2)
+        out = m.field()
+        if ref is None:
+            ref = out
+        np.testing.assert_array_equal(out, ref, err_msg=f"{c} columns, {r:#x} rows per CTA")
+        ran += 1
+    assert ran >= 6
+    for bad in ((3, 2), (4, 3), (4, 8), (16, 1), (4, 2 | 0x200)):
+        with pytest.raises(lb.LeniaError, match="unsupported launch shape"):
+            m.set_tuning(*bad)
+    m.close()
+    d = lb.LeniaModule(wl.fft3_params(w, h, conv="directMulti"), w, h)
+    assert d.tuning() == (0, 0)
+    with pytest.raises(lb.LeniaError):
+        d.set_tuning(4, 2)
+    d.close()
+
+
 def test_upload_download_roundtrip_and_device_copy():
     m = lb.LeniaModule({"radius": 4}, 37, 23)
     a = np.random.default_rng(3).random((23, 37)).astype(np.float32)
