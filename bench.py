@@ -33,6 +33,8 @@ pixels x steps; ``value`` is whole-job Mpixel-steps/s.
   stages (fp32 CUDA cores, fp16x3 / bf16x3 split-precision tensor cores);
   per-step device time, the column pass's HBM roofline and tensor FLOP rate
   (a radix-16 stage as a real 32x32 GEMM: 128 FLOP per point, x3 hi/lo).
+* library_fft_baseline: the same step from torch.fft (cuFFT) and torch ops
+  in one CUDA graph, same flush protocol: a library comparator.
 * --impl reference: that CPU reference alone, as the reference arm.
 """
 from __future__ import annotations
@@ -57,7 +59,7 @@ WORKLOAD = "fft3_1080p"
 FALLBACK_HBM_GBS = 6650.0
 # dram__bytes_read.sum + dram__bytes_write.sum per launch from one ncu
 # capture of the default workload (profiles/lenia_fft_step_1080p_k3.md).
-NCU_TRAFFIC_BYTES = {"row_growth": 33_256_704 + 5_632, "column": 14_575_104 + 5_376}
+NCU_TRAFFIC_BYTES = {"row_growth": 33_261_056 + 26_112, "column": 14_575_616 + 0}
 
 
 def parse_args():
@@ -76,6 +78,10 @@ def parse_args():
                          "on FP32 CUDA cores vs split-precision tensor cores")
     ap.add_argument("--adjoint-reps", type=int, default=5)
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-library-baseline", action="store_true")
+    ap.add_argument("--launch-shape", default=None,
+                    help="columns,rows per CTA of the two passes, e.g. 4,4p (p: pipelined rows); "
+                         "skips the shape search")
     ap.add_argument("--keep-tuning", action="store_true",
                     help="keep the setup autotuner's launch shapes instead of choosing them under the "
                          "bench's own conditions (flushed L2) before the timed region")
@@ -184,6 +190,71 @@ def cpu_baseline_port(params, w, h, init, seconds):
             break
     return {"value": w * h * steps / el / 1e6, "unit": UNIT, "cores": 1, "kind": "port",
             "sample": f"full {w}x{h} field, {steps} substeps in {el:.1f} s (FP64 oracle)"}
+
+
+def library_fft_baseline(params, w, h, init, steps: int = 50, warmup: int = 5) -> dict:
+    """The same step written with library FFTs: torch.fft (cuFFT) rfft2 of
+    the field, per kernel a product with its real spectrum and irfft2, the
+    growth sum, Euler step and clip in torch ops; the whole step captured
+    in one CUDA graph. Timed like the value region (L2 flushed before each
+    step, CUDA events around the graph replay). A comparator only: the
+    library's own kernels, none of this package's."""
+    import torch
+
+    K = len(params["kernels"])
+    r = float(params["radius"])
+    yy, xx = np.meshgrid(np.fft.fftfreq(h) * h, np.fft.fftfreq(w) * w, indexing="ij")
+    khat = []
+    for k in params["kernels"]:
+        # Ring image: exponential core exp(4 - 1/(s(1-s))) on each of the
+        # kernel's len(betas) shells of the normalised radius, peak beta_i.
+        d = np.sqrt(xx * xx + yy * yy) / (r * k.get("radiusScale", 1.0))
+        nb = len(k["betas"])
+        u = d * nb
+        i = np.minimum(np.floor(u), nb - 1).astype(int)
+        f = np.clip(u - i, 1e-6, 1 - 1e-6)
+        img = np.where(d < 1.0, np.array(k["betas"])[i] * np.exp(4.0 - 1.0 / (f * (1.0 - f))), 0.0)
+        img /= img.sum()
+        khat.append(torch.from_numpy(np.fft.rfft2(img).real.astype(np.float32)).cuda())
+    mu = [float(k["mu"]) for k in params["kernels"]]
+    sigma = [float(k["sigma"]) for k in params["kernels"]]
+    hw = [float(k["weight"]) for k in params["kernels"]]
+    dt = float(params["dt"])
+    state = torch.from_numpy(np.ascontiguousarray(init, dtype=np.float32)).cuda()
+    stream = torch.cuda.Stream()
+
+    def step():
+        fa = torch.fft.rfft2(state)
+        g = torch.zeros_like(state)
+        for q in range(K):
+            u = torch.fft.irfft2(fa * khat[q], s=state.shape)
+            g += hw[q] * (2.0 * torch.exp(-0.5 * ((u - mu[q]) / sigma[q]) ** 2) - 1.0)
+        state.copy_(torch.clamp(state + dt * g, 0.0, 1.0))
+
+    with torch.cuda.stream(stream):
+        for _ in range(3):
+            step()  # cuFFT plans made outside the capture
+    torch.cuda.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=stream):
+        step()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    times = []
+    with torch.cuda.stream(stream):
+        for i in range(warmup + steps):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            graph.replay()
+            b.record(stream)
+            if i >= warmup:
+                times.append((a, b))
+    torch.cuda.synchronize()
+    ms = float(np.mean([a.elapsed_time(b) for a, b in times]))
+    del graph
+    return {"what": "torch.fft (cuFFT) rfft2 + per kernel product and irfft2 + growth/Euler/clip in torch "
+                    "ops, one CUDA graph per step, L2 flushed before each step",
+            "ms_per_step": ms, "value": w * h / (ms / 1e3) / 1e6, "unit": UNIT, "steps": steps}
 
 
 def cpu_baseline(params, w, h, init, seconds):
@@ -297,7 +368,12 @@ def run_b200(args):
     # timing each supported shape outside the timed region; then the state
     # is reset so the timed steps start from the same field as without it.
     shape, chosen_by = m.tuning(), "setup autotuner"
-    if shape != (0, 0) and not args.keep_tuning:
+    if shape != (0, 0) and args.launch_shape:
+        c, r = args.launch_shape.split(",")
+        shape = (int(c), int(r.rstrip("p")) | (lb.ROWS_PIPELINED if r.endswith("p") else 0))
+        m.set_tuning(*shape)
+        chosen_by = "--launch-shape"
+    elif shape != (0, 0) and not args.keep_tuning:
         best = None
         for c in (8, 4, 2):
             for r in (4, 2, 1, 4 | lb.ROWS_PIPELINED, 2 | lb.ROWS_PIPELINED, 1 | lb.ROWS_PIPELINED):
@@ -399,6 +475,8 @@ def run_b200(args):
     })
     if rank == 0 and world == 1 and not args.no_adjoint:
         line["adjoint"] = adjoint_bench(args.adjoint_reps)
+    if rank == 0 and world == 1 and not args.no_library_baseline:
+        line["library_fft_baseline"] = library_fft_baseline(params, w, h, init)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_baseline(params, w, h, init, args.cpu_seconds)
