@@ -273,9 +273,12 @@ cudaError_t launch_chained(void (*fn)(KArgs...), dim3 grid, int threads, size_t 
 
 // Persistent grid over n worlds: grid.y = world, grid.x = CTAs per world
 // (the resident CTAs of the device shared out, at most one per group).
+// Rounded down: every CTA loops over its share of the pass, so a CTA beyond
+// the resident slots would wait for a whole persistent CTA to finish -- a
+// second wave as long as the first (e.g. 19 x 32 = 608 CTAs for 592 slots).
 inline dim3 world_grid(int per_sm, int groups, int n) {
     const int resident = std::max(1, per_sm) * sms();
-    const int x = std::max(1, std::min(groups, (resident + n - 1) / n));
+    const int x = std::max(1, std::min(groups, resident / std::max(1, n)));
     return dim3(unsigned(x), unsigned(n));
 }
 
