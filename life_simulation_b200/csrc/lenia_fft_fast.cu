@@ -51,6 +51,19 @@ using namespace fastfft;
 
 // ------------------------------------------------------------- columns
 
+// Shared-memory staging of the next column group's row spectrum (B columns
+// x H rows, row-major, 16-byte asynchronous copies): used when B is even and
+// the extra buffer fits the 227 KB a CTA may have.
+template <class PF, int B>
+struct ColStage {
+    using K = ColK<PF, B>;
+    static constexpr int OFF =
+        (PF::tw_size() + K::PI::tw_size() + 2 * B * K::PITCH + K::H + 1) / 2 * 2;  // 16-byte aligned
+    static constexpr size_t with_stage = sizeof(float2) * (size_t(OFF) + size_t(B) * K::H);
+    static constexpr bool on = B % 2 == 0 && with_stage <= 227 * 1024;
+    static constexpr size_t smem() { return on ? with_stage : K::smem(); }
+};
+
 template <class PF, int B>
 __global__ void __launch_bounds__(ColK<PF, B>::T)
     col_fast_kernel(SpectralWorld w0, const SpectralWorld* __restrict__ worlds,
@@ -75,19 +88,26 @@ __global__ void __launch_bounds__(ColK<PF, B>::T)
     float2* __restrict__ U = sw.U;
     const float* __restrict__ khat = sw.khat;
     const int M = sw.M, nk = sw.nk;
+    using CS = ColStage<PF, B>;
+    float2* bs = sm + CS::OFF;
+    // Rows of columns g0..g0+B-1 of S into bs as bs[i * B + b].
+    const auto stage_group = [&](int g0) {
+        const float2* src = S + size_t(g0 / KB) * H * KB + (g0 % KB);
+        for (int q = threadIdx.x; q < H * (B / 2); q += T) {
+            const int i = q / (B / 2), c2 = q - i * (B / 2);
+            cp_async16(bs + i * B + 2 * c2, src + size_t(i) * KB + 2 * c2);
+        }
+        cp_async_commit();
+    };
+    if constexpr (CS::on) {
+        if (int(blockIdx.x) * B < M) stage_group(int(blockIdx.x) * B);
+    }
     if (int(blockIdx.x) * B >= M) allow_dependents();
     for (int k0 = blockIdx.x * B; k0 < M; k0 += gridDim.x * B) {
         if (k0 + int(gridDim.x) * B >= M) allow_dependents();  // this CTA's last group
         const int cols = min(B, M - k0);
         // Element (b, ky) of this group in the blocked layout.
         const size_t gbase = size_t(k0 / KB) * H * KB + (k0 % KB);
-        pass_gen<PF, 0, false, B, T>([&](int b, int i) { return __ldg(S + gbase + size_t(i) * KB + b); },
-                                      [&](int b, int i, float2 v) { ba[b * PITCH + i] = v; }, twf, cols);
-        __syncthreads();
-        float2* X = mid_passes<PF, 1, PF::np - 1, false, B, T, PITCH>(ba, bb, twf, cols);
-        float2* Y = (X == ba) ? bb : ba;
-        // Last forward pass: the column spectrum C stays in registers.
-        float2 C[K::ITL][RL];
         int jj[K::ITL], bi[K::ITL];
         bool ok[K::ITL];
 #pragma unroll
@@ -96,6 +116,46 @@ __global__ void __launch_bounds__(ColK<PF, B>::T)
             jj[it] = q / B;
             bi[it] = q - jj[it] * B;
             ok[it] = q < B * NRL && bi[it] < cols;
+        }
+        // Kernel spectrum values of this thread's last-pass elements, one
+        // kernel ahead: kernel 0's are in flight during the forward
+        // transform, kernel k+1's during kernel k's inverse. kv2 is the
+        // Nyquist column's value, used by the packed column 0 only.
+        float kv[K::ITL][RL], kv2[K::ITL][RL];
+        const auto fetch_k = [&](int kk) {
+            const float* kh = khat + size_t(kk) * (M + 1) * Hh;
+#pragma unroll
+            for (int it = 0; it < K::ITL; ++it) {
+                const int kx = k0 + bi[it];
+#pragma unroll
+                for (int t = 0; t < RL; ++t) {
+                    const int ky = jj[it] + t * NRL;
+                    const int kyr = min(ky, H - ky);
+                    kv[it][t] = ok[it] ? __ldg(kh + size_t(kx) * Hh + kyr) : 0.0f;
+                    kv2[it][t] = (ok[it] && kx == 0) ? __ldg(kh + size_t(M) * Hh + kyr) : 0.0f;
+                }
+            }
+        };
+        if (nk > 0) fetch_k(0);
+        if constexpr (CS::on) {
+            cp_async_wait_all();
+            __syncthreads();  // this group's rows staged
+            pass_gen<PF, 0, false, B, T>([&](int b, int i) { return bs[i * B + b]; },
+                                          [&](int b, int i, float2 v) { ba[b * PITCH + i] = v; }, twf, cols);
+            __syncthreads();  // bs read: the next group's rows may land
+            const int next = k0 + int(gridDim.x) * B;
+            if (next < M) stage_group(next);
+        } else {
+            pass_gen<PF, 0, false, B, T>([&](int b, int i) { return __ldg(S + gbase + size_t(i) * KB + b); },
+                                          [&](int b, int i, float2 v) { ba[b * PITCH + i] = v; }, twf, cols);
+            __syncthreads();
+        }
+        float2* X = mid_passes<PF, 1, PF::np - 1, false, B, T, PITCH>(ba, bb, twf, cols);
+        float2* Y = (X == ba) ? bb : ba;
+        // Last forward pass: the column spectrum C stays in registers.
+        float2 C[K::ITL][RL];
+#pragma unroll
+        for (int it = 0; it < K::ITL; ++it) {
             if (ok[it]) {
 #pragma unroll
                 for (int t = 0; t < RL; ++t) C[it][t] = X[bi[it] * PITCH + IL::in(jj[it], t)];
@@ -109,7 +169,6 @@ __global__ void __launch_bounds__(ColK<PF, B>::T)
         }
         if (k0 == 0) __syncthreads();  // c0 (packed DC/Nyquist column) visible
         for (int kk = 0; kk < nk; ++kk) {
-            const float* kh = khat + size_t(kk) * (M + 1) * Hh;
             // Spectrum product, then the inverse's first pass (radix RL, no
             // twiddles) from registers into Y.
 #pragma unroll
@@ -120,19 +179,19 @@ __global__ void __launch_bounds__(ColK<PF, B>::T)
 #pragma unroll
                 for (int t = 0; t < RL; ++t) {
                     const int ky = jj[it] + t * NRL;
-                    const int kyr = min(ky, H - ky);
                     if (kx == 0) {
-                        const float P = __ldg(kh + kyr), Q = __ldg(kh + size_t(M) * Hh + kyr);
+                        const float P = kv[it][t], Q = kv2[it][t];
                         const float2 Cm = cconj(c0[ky == 0 ? 0 : H - ky]);
                         D[t] = cadd(cscale(C[it][t], 0.5f * (P + Q)), cscale(Cm, 0.5f * (P - Q)));
                     } else {
-                        D[t] = cscale(C[it][t], __ldg(kh + size_t(kx) * Hh + kyr));
+                        D[t] = cscale(C[it][t], kv[it][t]);
                     }
                 }
                 Dft<RL, true>::run(D);
 #pragma unroll
                 for (int t = 0; t < RL; ++t) Y[bi[it] * PITCH + jj[it] * RL + t] = D[t];
             }
+            if (kk + 1 < nk) fetch_k(kk + 1);
             __syncthreads();
             float2* Z = mid_passes<PI, 1, PI::np - 1, true, B, T, PITCH>(Y, X, twi, cols);
             float2* dst = U + size_t(kk) * M * H + gbase;
@@ -343,7 +402,7 @@ cudaError_t launch_col_t(const SpectralWorld& w0, const SpectralWorld* worlds, i
                          const FastTables& t, cudaStream_t s) {
     using K = ColK<PF, B>;
     auto fn = col_fast_kernel<PF, B>;
-    const size_t smem = K::smem();
+    const size_t smem = ColStage<PF, B>::smem();
     if (smem > 227 * 1024 || K::T > 1024) return cudaErrorInvalidConfiguration;
     cudaError_t e = prepare(fn, smem);
     if (e != cudaSuccess) return e;
@@ -459,7 +518,7 @@ cudaError_t row_dispatch(int H, int M, int batch, const SpectralWorld& w0, const
 template <class PF, int B>
 bool col_shape_ok() {
     using K = ColK<PF, B>;
-    return K::T <= 1024 && K::smem() <= 227 * 1024;
+    return K::T <= 1024 && ColStage<PF, B>::smem() <= 227 * 1024;
 }
 
 template <class PI, int RB, bool PIPE>
