@@ -311,8 +311,15 @@ template <class PF, int B>
 struct ColAdjK {
     using K = ColK<PF, B>;
     // ColK's buffers (twiddles, two work buffers, one packed column) plus a
-    // second packed column (A's).
-    static constexpr size_t smem() { return K::smem() + sizeof(float2) * size_t(K::H); }
+    // second packed column (A's), then (when B is even and it fits) a staging
+    // buffer of B columns x H rows for the next first-pass input.
+    static constexpr int OFF =
+        (PF::tw_size() + K::PI::tw_size() + 2 * B * K::PITCH + 2 * K::H + 1) / 2 * 2;  // 16-byte aligned
+    static constexpr size_t with_stage = sizeof(float2) * (size_t(OFF) + size_t(B) * K::H);
+    static constexpr bool stage = B % 2 == 0 && with_stage <= 227 * 1024;
+    static constexpr size_t smem() {
+        return stage ? with_stage : K::smem() + sizeof(float2) * size_t(K::H);
+    }
 };
 
 template <class PF, int B>
@@ -339,6 +346,47 @@ __global__ void __launch_bounds__(ColK<PF, B>::T)
     __syncthreads();
     const int M = a.M, nk = a.nk;
     const bool beta = a.ntab > 0 && sw.S != nullptr;
+    // First-pass inputs of a column group, in order: A_t's row spectrum
+    // (with beta), then SQ_0 .. SQ_{nk-1}. With staging, input j + 1 (or the
+    // next group's first) is copied into bs by cp.async while input j is
+    // transformed.
+    using CAK = ColAdjK<PF, B>;
+    float2* bs = sm + CAK::OFF;
+    const int nin = nk + (beta ? 1 : 0);
+    const auto input_plane = [&](int j) -> const float2* {
+        return beta ? (j == 0 ? sw.S : sw.SQ + size_t(j - 1) * M * H) : sw.SQ + size_t(j) * M * H;
+    };
+    const auto stage_input = [&](int g0, int j) {
+        const float2* src = input_plane(j) + size_t(g0 / KB) * H * KB + (g0 % KB);
+        for (int q = threadIdx.x; q < H * (B / 2); q += T) {
+            const int i = q / (B / 2), c2 = q - i * (B / 2);
+            cp_async16(bs + i * B + 2 * c2, src + size_t(i) * KB + 2 * c2);
+        }
+        cp_async_commit();
+    };
+    // Forward column FFT of the group's input j up to its last pass (which
+    // the caller runs into registers); returns the buffer holding the last
+    // pass's input.
+    const auto forward_input = [&](int k0, int j, int cols) -> float2* {
+        if constexpr (CAK::stage) {
+            cp_async_wait_all();
+            __syncthreads();  // input j staged
+            pass_gen<PF, 0, false, B, T>([&](int b, int i) { return bs[i * B + b]; },
+                                          [&](int b, int i, float2 v) { ba[b * PITCH + i] = v; }, twf, cols);
+            __syncthreads();  // bs read
+            if (j + 1 < nin)
+                stage_input(k0, j + 1);
+            else if (k0 + int(gridDim.x) * B < M)
+                stage_input(k0 + int(gridDim.x) * B, 0);
+            return mid_passes<PF, 1, PF::np - 1, false, B, T, PITCH>(ba, bb, twf, cols);
+        } else {
+            return col_forward<PF, B, T, PITCH>(input_plane(j) + size_t(k0 / KB) * H * KB + (k0 % KB), ba, bb, twf,
+                                                cols);
+        }
+    };
+    if constexpr (CAK::stage) {
+        if (int(blockIdx.x) * B < M && nin > 0) stage_input(int(blockIdx.x) * B, 0);
+    }
     for (int k0 = blockIdx.x * B; k0 < M; k0 += gridDim.x * B) {
         const int cols = min(B, M - k0);
         const size_t gbase = size_t(k0 / KB) * H * KB + (k0 % KB);
@@ -351,6 +399,24 @@ __global__ void __launch_bounds__(ColK<PF, B>::T)
             bi[it] = q - jj[it] * B;
             ok[it] = q < B * NRL && bi[it] < cols;
         }
+        // Kernel spectrum values of this thread's elements, one kernel
+        // ahead (kv2: the Nyquist column's value, for the packed column 0).
+        float kv[ITL][RL], kv2[ITL][RL];
+        const auto fetch_k = [&](int kk) {
+            const float* kh = a.khat + size_t(kk) * (M + 1) * Hh;
+#pragma unroll
+            for (int it = 0; it < ITL; ++it) {
+                const int kx = k0 + bi[it];
+#pragma unroll
+                for (int t = 0; t < RL; ++t) {
+                    const int ky = jj[it] + t * NRL;
+                    const int kyr = min(ky, H - ky);
+                    kv[it][t] = ok[it] ? __ldg(kh + size_t(kx) * Hh + kyr) : 0.0f;
+                    kv2[it][t] = (ok[it] && kx == 0) ? __ldg(kh + size_t(M) * Hh + kyr) : 0.0f;
+                }
+            }
+        };
+        if (nk > 0) fetch_k(0);
         // Last forward pass of a column FFT into registers (+ packed column).
         const auto last_pass = [&](const float2* X, float2 (&C)[ITL][RL], float2* c0) {
 #pragma unroll
@@ -368,17 +434,16 @@ __global__ void __launch_bounds__(ColK<PF, B>::T)
         };
         float2 Ah[ITL][RL];
         if (beta) {
-            float2* X = col_forward<PF, B, T, PITCH>(sw.S + gbase, ba, bb, twf, cols);
+            float2* X = forward_input(k0, 0, cols);
             last_pass(X, Ah, c0a);
             __syncthreads();  // X read
         }
         float2 G[ITL][RL];
         for (int kk = 0; kk < nk; ++kk) {
             float2 Q[ITL][RL];
-            float2* X = col_forward<PF, B, T, PITCH>(sw.SQ + size_t(kk) * M * H + gbase, ba, bb, twf, cols);
+            float2* X = forward_input(k0, kk + (beta ? 1 : 0), cols);
             last_pass(X, Q, c0q);
             __syncthreads();  // X read; packed columns visible
-            const float* kh = a.khat + size_t(kk) * (M + 1) * Hh;
 #pragma unroll
             for (int it = 0; it < ITL; ++it) {
                 if (!ok[it]) continue;
@@ -386,18 +451,18 @@ __global__ void __launch_bounds__(ColK<PF, B>::T)
 #pragma unroll
                 for (int t = 0; t < RL; ++t) {
                     const int ky = jj[it] + t * NRL;
-                    const int kyr = min(ky, H - ky);
                     float2 D;
                     if (kx == 0) {
-                        const float P = __ldg(kh + kyr), Qn = __ldg(kh + size_t(M) * Hh + kyr);
+                        const float P = kv[it][t], Qn = kv2[it][t];
                         const float2 Cm = cconj(c0q[ky == 0 ? 0 : H - ky]);
                         D = cadd(cscale(Q[it][t], 0.5f * (P + Qn)), cscale(Cm, 0.5f * (P - Qn)));
                     } else {
-                        D = cscale(Q[it][t], __ldg(kh + size_t(kx) * Hh + kyr));
+                        D = cscale(Q[it][t], kv[it][t]);
                     }
                     G[it][t] = kk == 0 ? D : cadd(G[it][t], D);
                 }
             }
+            if (kk + 1 < nk) fetch_k(kk + 1);
             if (beta) {
                 for (int tb = 0; tb < a.ntab; ++tb) {
                     if (a.tab_kernel[tb] != kk) continue;
