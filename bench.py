@@ -416,6 +416,30 @@ def run_b200(args):
         total_ms = float(t.item())
     value = world * w * h * args.steps / (total_ms / 1e3) / 1e6
 
+    # A frame with its colour layer (RGBA16F at the sim size): lenia_step +
+    # lenia_render_rgba16f against lenia_step_render, which writes the texels
+    # from the last substep's row pass. Flushed, CUDA events, same stream.
+    rgba = torch.empty((h, w, 4), dtype=torch.float16, device="cuda")
+    frame_ms = {}
+    for mode in ("separate", "fused", "separate", "fused"):
+        evs = []
+        for i in range(40):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            if mode == "fused":
+                m.step_render(fp, 1, rgba.data_ptr(), w, h, sh)
+            else:
+                m.step(fp, 1, sh)
+                m.render_device(rgba.data_ptr(), w, h, sh)
+            b.record(stream)
+            if i >= 5:
+                evs.append((a, b))
+        barrier()
+        frame_ms[mode] = statistics.median(x.elapsed_time(y) for x, y in evs)
+    render_line = {"what": "one substep + the RGBA16F colour layer at the sim size per frame, L2 flushed",
+                   "separate_ms": frame_ms["separate"], "fused_ms": frame_ms["fused"]}
+
     # End to end through the C ABI with pinned host buffers.
     e2e_steps = args.e2e_steps or max(10, args.steps // 4)
     host_in = torch.empty((h, w), dtype=torch.float32, pin_memory=True).numpy()
@@ -471,6 +495,7 @@ def run_b200(args):
                               "frac": step_bytes / (mean_step_ms / 1e3) / 1e9 / peak}},
         "phases_ms_per_step": {k: v["ms"] / prof_steps for k, v in phases.items()},
         "kernel_timing": f"per-launch CUDA events over {prof_steps} further flushed steps",
+        "frame_with_colour_layer": render_line,
         "clocks": cl,
     })
     if rank == 0 and world == 1 and not args.no_adjoint:

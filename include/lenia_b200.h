@@ -263,6 +263,16 @@ int lenia_colormap_from_json(const char* params_json, lenia_colormap* out);
  * the module's output at the scene resolution (Lenia.cpp:646-652).
  * Asynchronous on `stream` after the queued steps. */
 int lenia_render_rgba16f(lenia_ctx* ctx, void* dst, uint32_t width, uint32_t height, void* stream);
+/* lenia_step followed by lenia_render_rgba16f of the new field, with the
+ * colour pass fused into the last substep where it can be (extension; the
+ * reference encodes the step and then colorMapField, Lenia.cpp:562-652):
+ * when width x height is the sim size, the context is on the compile-time-
+ * plan spectral path and dst is 16-byte aligned, the last substep's row
+ * pass writes the texels from the values it has just computed, saving the
+ * colour pass's re-read of the field and its launch. Otherwise the two run
+ * in turn. The texels are the same either way. */
+int lenia_step_render(lenia_ctx* ctx, const lenia_frame_params* fp, uint32_t substeps, void* dst, uint32_t width,
+                      uint32_t height, void* stream);
 
 /* ---- Many worlds at once (batched sweep) ----
  * Replaces the reference's one-world-at-a-time variant loop

@@ -105,6 +105,7 @@ EXPORTS = (
     "lenia_bus_set_section", "lenia_bus_clear_features", "lenia_bus_update", "lenia_bus_value",
     "lenia_bus_last_message", "lenia_create_scene_module", "lenia_attach_bus",
     "lenia_get_colormap", "lenia_set_colormap", "lenia_colormap_from_json", "lenia_render_rgba16f",
+    "lenia_step_render",
     "lenia_batch_init_noise", "lenia_batch_activity",
     "lenia_npy_write_f32", "lenia_npy_read_f32", "lenia_save_state", "lenia_load_state",
 )
@@ -248,6 +249,7 @@ def load_library(path: str = LIB_PATH):
     L.lenia_set_colormap.argtypes = [P, ctypes.POINTER(ColorMap)]
     L.lenia_colormap_from_json.argtypes = [ctypes.c_char_p, ctypes.POINTER(ColorMap)]
     L.lenia_render_rgba16f.argtypes = [P, P, u32, u32, P]
+    L.lenia_step_render.argtypes = [P, ctypes.POINTER(FrameParams), u32, P, u32, u32, P]
     L.lenia_batch_init_noise.argtypes = [P, u32, u32, ctypes.c_float, ctypes.c_float]
     L.lenia_npy_write_f32.argtypes = [ctypes.c_char_p, P, ctypes.c_size_t, P, u32]
     L.lenia_npy_read_f32.argtypes = [ctypes.c_char_p, P, u32, P, ctypes.c_size_t]
@@ -424,6 +426,14 @@ class LeniaModule:
         """Colour layer (RGBA16F, 8 bytes per pixel) into a device buffer."""
         self._check(self._L.lenia_render_rgba16f(self._h, ctypes.c_void_p(ptr), width, height,
                                                  ctypes.c_void_p(stream) if stream else None))
+
+    def step_render(self, fp: "FrameParams", substeps: int, ptr: int, width: int, height: int,
+                    stream: Optional[int] = None) -> None:
+        """step() then the colour layer of the new field into a device
+        buffer; at the sim size on the spectral path the last substep writes
+        it directly (no separate colour pass). Same texels as render_device."""
+        self._check(self._L.lenia_step_render(self._h, ctypes.byref(fp), substeps, ctypes.c_void_p(ptr), width,
+                                              height, ctypes.c_void_p(stream) if stream else None))
 
     def save_state(self, path: str) -> None:
         """The field as a (height, width) float32 .npy file."""

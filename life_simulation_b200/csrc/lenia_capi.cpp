@@ -408,6 +408,18 @@ int lenia_render_rgba16f(lenia_ctx* c, void* dst, uint32_t width, uint32_t heigh
     });
 }
 
+int lenia_step_render(lenia_ctx* c, const lenia_frame_params* fp, uint32_t substeps, void* dst, uint32_t width,
+                      uint32_t height, void* stream) {
+    if (!c || !fp) return LENIA_ERR_INVALID_ARG;
+    if (!(fp->growth_sigma != 0.0f)) {
+        c->message = "growth_sigma must be nonzero";
+        return LENIA_ERR_INVALID_ARG;
+    }
+    return guarded(c, [&] {
+        return set_msg(c, c->module.stepRender(*fp, substeps, dst, width, height, static_cast<cudaStream_t>(stream)));
+    });
+}
+
 // ---------------------------------------------------------- state files
 
 int lenia_npy_write_f32(const char* path, const float* data, size_t count, const uint32_t* shape, uint32_t ndim) {

@@ -32,6 +32,7 @@
 #include <vector>
 
 #include "fft_ct.cuh"
+#include "colormap.cuh"
 #include "fft_fast_common.cuh"
 #include "lenia_device.cuh"
 #include "lenia_kernels.h"
@@ -205,6 +206,21 @@ __global__ void __launch_bounds__(ColK<PF, B>::T)
 
 // ---------------------------------------------------------------- rows
 
+// The colour layer of two adjacent pixels of A' (the module's output pass,
+// fused into the last substep): both RGBA16F texels in one 16-byte store.
+// Out of line: the rare path costs the row pass no registers.
+static __device__ __noinline__ void palette_pair(const ColorMapParams& cm, float2 v, uint2* dst) {
+    __half t0[4], t1[4];
+    palette_rgba16f(cm, channel_of(v.x, cm.channel), t0);
+    palette_rgba16f(cm, channel_of(v.y, cm.channel), t1);
+    uint4 q;
+    q.x = uint32_t(__half_as_ushort(t0[0])) | (uint32_t(__half_as_ushort(t0[1])) << 16);
+    q.y = uint32_t(__half_as_ushort(t0[2])) | (uint32_t(__half_as_ushort(t0[3])) << 16);
+    q.z = uint32_t(__half_as_ushort(t1[0])) | (uint32_t(__half_as_ushort(t1[1])) << 16);
+    q.w = uint32_t(__half_as_ushort(t1[2])) | (uint32_t(__half_as_ushort(t1[3])) << 16);
+    *reinterpret_cast<uint4*>(dst) = q;
+}
+
 // nk > 0: inverse row transforms of U_k, growth, A' (+ the next step's row
 // spectrum when S_next != null). nk == 0: only the forward row transform of
 // A into S_next (the first step after an upload or init).
@@ -361,6 +377,7 @@ __global__ void __launch_bounds__(RowK<PI, RB>::T, (512 / RowK<PI, RB>::T > 1 ? 
                                 growth_finish_lean(p, a.y, acc[it][t][1], acc[it][t][1], uint32_t(2 * n + 1),
                                                    uint32_t(gy)));
                 *reinterpret_cast<float2*>(A_out + size_t(gy) * W + 2 * n) = r;
+                if (sw.rgba) palette_pair(sw.cm, r, sw.rgba + size_t(gy) * W + 2 * n);
                 za[it][t] = r;
             }
         }
@@ -575,8 +592,12 @@ cudaError_t launch_col_fast(const FftGeometry& g, const FastTables& t, int batch
 
 cudaError_t launch_row_fast(const FftGeometry& g, const FastTables& t, int batch, const float2* U,
                             const float* A, float* A_out, float2* S_next, const StepParams& p,
-                            int nk, cudaStream_t s) {
+                            int nk, cudaStream_t s, void* rgba16f, const ColorMapParams* cm) {
     SpectralWorld w{};
+    if (rgba16f && cm && nk > 0) {
+        w.rgba = static_cast<uint2*>(rgba16f);
+        w.cm = *cm;
+    }
     w.U = const_cast<float2*>(U);  // read only by the row pass
     w.A = A;
     w.A_out = A_out;

@@ -98,6 +98,11 @@ struct FastTables {
 };
 // One world of a spectral pass launch. A launch covers one world (passed by
 // value) or a table of worlds of the same size (blockIdx.y = world index).
+struct ColorMapParams {  // ColorMapParams, Shaders/Render/ColorMap.metal:6-15
+    float a[3], b[3], c[3], d[3];
+    float input_scale, input_bias, exposure;
+    uint32_t channel;
+};
 struct SpectralWorld {
     const float2* S;     // row spectrum of A (blocked layout)
     float2* U;           // nk potential spectra (blocked layout)
@@ -106,9 +111,11 @@ struct SpectralWorld {
     float* A_out;        // state out
     float2* S_next;      // row spectrum of A_out, or null
     float* U_px;         // row pass: nk potential planes (H x W) to keep, or null
+    uint2* rgba;         // row pass: the colour layer of A_out (H x W RGBA16F texels), or null
     int M;               // columns of the half spectrum (W/2)
     int nk;              // kernels (0: row pass computes only S_next of A)
     StepParams p;
+    ColorMapParams cm;   // palette of `rgba`
 };
 
 bool fast_col_plan(int H, FastPlan& forward_plan);
@@ -135,7 +142,7 @@ cudaError_t launch_col_fast(const FftGeometry& g, const FastTables& t, int batch
                             float2* U, cudaStream_t s);
 cudaError_t launch_row_fast(const FftGeometry& g, const FastTables& t, int batch, const float2* U,
                             const float* A, float* A_out, float2* S_next, const StepParams& p,
-                            int nk, cudaStream_t s);
+                            int nk, cudaStream_t s, void* rgba16f = nullptr, const ColorMapParams* cm = nullptr);
 // Many worlds of one size (W = 2M, H) in one launch per pass: `worlds` is a
 // device array of n entries; H, M select the compile-time plans. tw_r2c:
 // exp(-2 pi i k / W), k <= M (device).
@@ -154,11 +161,6 @@ cudaError_t launch_col_tc(const FftGeometry& g, const FastTables& t, int precisi
 
 // Colour map (lenia_colormap.cu): the field (w x h) to ow x oh RGBA16F
 // (ushort4 per pixel); bilinear with wrapping when the sizes differ.
-struct ColorMapParams {  // ColorMapParams, Shaders/Render/ColorMap.metal:6-15
-    float a[3], b[3], c[3], d[3];
-    float input_scale, input_bias, exposure;
-    uint32_t channel;
-};
 cudaError_t launch_colormap(const float* field, int w, int h, const ColorMapParams& p, void* rgba16f, int ow,
                             int oh, cudaStream_t s);
 

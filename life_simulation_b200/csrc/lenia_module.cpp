@@ -1118,6 +1118,23 @@ void LeniaModule::fillStepParams(const lenia_frame_params& fp, uint32_t seed, St
 }
 
 int LeniaModule::step(const lenia_frame_params& fp, uint32_t substeps, cudaStream_t stream) {
+    return stepImpl(fp, substeps, stream, nullptr);
+}
+
+int LeniaModule::stepRender(const lenia_frame_params& fp, uint32_t substeps, void* rgba16f, uint32_t dst_w,
+                            uint32_t dst_h, cudaStream_t stream) {
+    if (!rgba16f || dst_w == 0 || dst_h == 0) return fail(LENIA_ERR_INVALID_ARG, "render: null buffer or empty size");
+    if (!field_[0]) return fail(LENIA_ERR_STATE, "module is not set up");
+    const bool fused = use_fft_ && fast_row_ && dst_w == w_ && dst_h == h_ &&
+                       (reinterpret_cast<uintptr_t>(rgba16f) & 15u) == 0;
+    const int rc = stepImpl(fp, substeps, stream, fused ? rgba16f : nullptr);
+    if (rc < 0 || fused) return rc;
+    return render(rgba16f, dst_w, dst_h, stream ? stream : stream_);
+}
+
+// `rgba16f` (or null): the last substep's row pass also writes the colour
+// layer of its result at the sim size.
+int LeniaModule::stepImpl(const lenia_frame_params& fp, uint32_t substeps, cudaStream_t stream, void* rgba16f) {
     if (!field_[0]) return fail(LENIA_ERR_STATE, "module is not set up");
     cudaStream_t s = stream ? stream : stream_;
     int rc;
@@ -1153,8 +1170,10 @@ int LeniaModule::step(const lenia_frame_params& fp, uint32_t substeps, cudaStrea
                                  : launch_col_conv(fgeo_, d_S_, d_U_, s);
             });
             if (e != cudaSuccess) return cudaFail(e, "column pass");
+            void* out_rgba = i + 1 == n ? rgba16f : nullptr;
             e = launch(LENIA_PHASE_ROW_GROWTH, s, [&] {
-                return fast_row_ ? launch_row_fast(fgeo_, fast_, row_batch_, d_U_, src, dst, d_S_, p, fgeo_.nk, s)
+                return fast_row_ ? launch_row_fast(fgeo_, fast_, row_batch_, d_U_, src, dst, d_S_, p, fgeo_.nk, s,
+                                                   out_rgba, &colormap_)
                                  : launch_row_c2r_growth(fgeo_, d_U_, src, dst, d_S_, p, s);
             });
             if (e != cudaSuccess) return cudaFail(e, "growth pass");

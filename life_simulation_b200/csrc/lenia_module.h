@@ -97,6 +97,12 @@ public:
                cudaStream_t stream);
     // encode with explicit per-frame values.
     int step(const lenia_frame_params& fp, uint32_t substeps, cudaStream_t stream);
+    // step, then the colour layer of the new field into a dst_w x dst_h
+    // RGBA16F buffer. At the sim size on the compile-time-plan spectral path
+    // the last substep's row pass writes it (no separate colour pass); other
+    // sizes and paths run render() after the step. Same texels either way.
+    int stepRender(const lenia_frame_params& fp, uint32_t substeps, void* rgba16f, uint32_t dst_w, uint32_t dst_h,
+                   cudaStream_t stream);
     // Per-frame values as encode would read them (Lenia.cpp:456-464).
     lenia_frame_params resolveFrameParams(const ParameterBus& params, uint32_t frame_index,
                                           uint32_t audio_frame) const;
@@ -141,6 +147,7 @@ private:
     int buildDirectTables();
     int buildSpectralTables(const std::vector<KernelDef>& eff);
     int autotuneSpectral();
+    int stepImpl(const lenia_frame_params& fp, uint32_t substeps, cudaStream_t stream, void* rgba16f);
     int initField(const lenia_frame_params& fp, cudaStream_t s);
     int initKernels(const lenia_frame_params& fp);
     void fillStepParams(const lenia_frame_params& fp, uint32_t seed, StepParams& p) const;

@@ -64,3 +64,45 @@ def test_render_same_size_on_the_fft_path_and_profile():
     ref = ref_colormap(m.field(), m.colormap().as_dict(), w, h)
     assert half_ulps(out.cpu().numpy()[..., :3], ref[..., :3]) <= 1
     m.close()
+
+
+@pytest.mark.parametrize("pal", [0, 2, 3])
+@pytest.mark.parametrize("case", ["fft3_1080p", "fft_128x64", "direct_64x48", "fft_rescaled"])
+def test_fused_step_render_equals_step_then_render(pal, case):
+    """lenia_step_render (the colour pass fused into the last substep's row
+    pass where it can be) gives the same field and the same texels as
+    lenia_step followed by lenia_render_rgba16f."""
+    if case == "fft3_1080p":
+        params, w, h, init = wl.workload("fft3_1080p")
+        ow, oh = w, h
+    elif case == "fft_128x64":
+        w, h = 128, 64
+        params, init = wl.fft3_params(w, h), wl.patches(w, h, 6, 24, seed=5)
+        params["radius"] = 12
+        ow, oh = w, h
+    elif case == "direct_64x48":
+        w, h = 64, 48
+        params, init = {"radius": 8}, wl.patches(w, h, 4, 16, seed=6)
+        ow, oh = w, h
+    else:
+        w, h = 128, 64
+        params, init = wl.fft3_params(w, h), wl.patches(w, h, 6, 24, seed=5)
+        params["radius"] = 12
+        ow, oh = 200, 90
+    params = dict(params, noiseAmount=0.05, **PALETTES[pal])
+    a, b = lb.LeniaModule(params, w, h), lb.LeniaModule(params, w, h)
+    out_a = torch.zeros((oh, ow, 4), dtype=torch.float16, device="cuda")
+    out_b = torch.ones((oh, ow, 4), dtype=torch.float16, device="cuda")
+    for m in (a, b):
+        m.reset(4)
+        m.upload(init)
+    for f in range(2):  # two frames in a row: the fused texels follow each step
+        fa, fb = a.frame_params(f), b.frame_params(f)
+        a.step_render(fa, 2, out_a.data_ptr(), ow, oh)
+        b.step(fb, 2)
+        b.render_device(out_b.data_ptr(), ow, oh)
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(a.field(), b.field())
+        assert torch.equal(out_a.view(torch.int16), out_b.view(torch.int16)), (case, pal, f)
+    a.close()
+    b.close()
