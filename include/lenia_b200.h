@@ -127,6 +127,7 @@ typedef struct lenia_info {
     uint64_t device_bytes;    /* device memory held by the context */
     uint32_t fft_radix_row[8], fft_radix_col[8]; /* FFT plans (0-terminated) */
     uint32_t fft_precision;   /* LENIA_FFT_* of the column DFT stages in use */
+    uint32_t direct_tma;      /* 1: the direct path loads interior halo tiles by TMA */
 } lenia_info;
 
 typedef struct lenia_ctx lenia_ctx;

@@ -249,7 +249,7 @@ int lenia_sync(lenia_ctx* c) {
         c->message = std::string("device error: ") + cudaGetErrorString(e);
         return LENIA_ERR_CUDA;
     }
-    return LENIA_OK;
+    return guarded(c, [&] { return set_msg(c, c->module.checkDeviceFlags()); });
 }
 
 int lenia_field_size(lenia_ctx* c, uint32_t* w, uint32_t* h) {

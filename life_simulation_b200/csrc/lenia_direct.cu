@@ -6,7 +6,9 @@
 // Design (FP32 CUDA cores; the op is 2*nnz FLOP per pixel against 8 bytes
 // of state, so it is compute-bound):
 //   * a CTA owns a TW x TH output tile; the (TH+2R) x (TW+2R) halo tile is
-//     staged once in shared memory with toroidal wrap folded into the load;
+//     staged once in shared memory: by one TMA box load (cp.async.bulk.tensor,
+//     completion on an mbarrier) when the box lies inside the field, else by
+//     element loads with the toroidal wrap folded into the index;
 //   * every thread owns 8 consecutive outputs of one row and walks the
 //     kernel row by row; along x it consumes 8 taps at a time: 4 LDS.128 of
 //     inputs and 2 LDS.128 of (warp-uniform, broadcast) weights feed 64 FFMA,
@@ -17,9 +19,12 @@
 //     ascending dy (the reference's order);
 //   * the growth map, Euler step, noise, blob injection and clip run on the
 //     accumulators before the single store of A'.
+#include <cuda.h>  // CUtensorMap and its encoding enums (the driver entry point is fetched at run time)
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <cstring>
 
 #include "lenia_device.cuh"
 #include "lenia_kernels.h"
@@ -43,13 +48,53 @@ __device__ __forceinline__ void unpack_span(uint32_t v, int& start, int& count) 
     count = int(v >> 16);
 }
 
-// One output tile at (x0, y0) of one world.
+// --- TMA halo load (sm_90+ PTX: mbarrier + cp.async.bulk.tensor) ---------
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+// Makes the initialised barrier visible to the asynchronous (TMA) proxy.
+__device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory"); }
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Box (x, y) of a 2D tensor map into shared memory; x (the innermost
+// coordinate) is a multiple of 4 floats, as a TMA copy requires.
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::
+            "r"(smem_addr(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_addr(bar))
+        : "memory");
+}
+// Polls of the halo-load barrier before a CTA gives up (the load of a few
+// tens of KB lands within microseconds; this bound is reached only if the
+// device stops delivering it).
+constexpr uint32_t kTmaPolls = 1u << 22;
+
+// One output tile at (x0, y0) of one world. `tmap` (or null): the state's
+// halo-tile tensor map; `err` counts halo loads whose wait ran out.
 template <int TW, int TH, int NK>
 __device__ __forceinline__ void direct_tile(const float* __restrict__ src, float* __restrict__ dst,
                                             const float* __restrict__ weights,  // [NK][2R+1][WP], zero padded
                                             const uint32_t* __restrict__ spans, // [NK][2R+1]
-                                            const DirectGeometry& g, const StepParams& p, int x0, int y0) {
-    extern __shared__ __align__(16) float smem[];
+                                            const DirectGeometry& g, const StepParams& p, int x0, int y0,
+                                            const CUtensorMap* tmap, int* err) {
+    extern __shared__ __align__(128) float smem[];
+    __shared__ __align__(8) uint64_t tma_bar;
     const int TP = TW + 2 * g.xp + 8;          // tile pitch (floats), multiple of 4
     const int TR = TH + 2 * g.r;               // tile rows
     float* tile = smem;                        // [TR][TP]
@@ -61,19 +106,48 @@ __device__ __forceinline__ void direct_tile(const float* __restrict__ src, float
     constexpr int NT = DirectTile<TW, TH>::kThreads;
 
     // Stage the halo tile: tile[r][c] = A[(y0 - R + r) mod H][(x0 - XP + c) mod W].
-    for (int i = tid; i < TR * TP; i += NT) {
-        int r = i / TP, c = i - r * TP;
-        int gy = y0 - g.r + r;
-        int gx = x0 - g.xp + c;
-        gy %= H;
-        if (gy < 0) gy += H;
-        gx %= W;
-        if (gx < 0) gx += W;
-        tile[i] = __ldg(src + size_t(gy) * W + gx);
+    // A box inside the field is one TMA load (its TR x TP layout is the
+    // tile's); a box that wraps around the torus is loaded element by element.
+    const int bx = x0 - g.xp, by = y0 - g.r;
+    const bool tma = tmap != nullptr && bx >= 0 && bx + TP <= W && by >= 0 && by + TR <= H &&
+                     (smem_addr(tile) & 127u) == 0u;
+    if (tma) {
+        if (tid == 0) {
+            mbar_init(&tma_bar, 1);
+            mbar_init_fence();
+        }
+        __syncthreads();
+        if (tid == 0) {
+            mbar_arrive_expect_tx(&tma_bar, uint32_t(TR * TP) * uint32_t(sizeof(float)));
+            tma_load_2d(tile, tmap, bx, by, &tma_bar);
+        }
+    } else {
+        for (int i = tid; i < TR * TP; i += NT) {
+            int r = i / TP, c = i - r * TP;
+            int gy = y0 - g.r + r;
+            int gx = x0 - g.xp + c;
+            gy %= H;
+            if (gy < 0) gy += H;
+            gx %= W;
+            if (gx < 0) gx += W;
+            tile[i] = __ldg(src + size_t(gy) * W + gx);
+        }
     }
     const int nw = NK * g.ksize * g.wp;
     for (int i = tid; i < nw; i += NT) wts[i] = __ldg(weights + i);
     for (int i = tid; i < NK * g.ksize; i += NT) sp[i] = __ldg(spans + i);
+    if (tma) {
+        bool done = false;
+        for (uint32_t i = 0; i < kTmaPolls && !done; ++i) done = mbar_try_wait(&tma_bar, 0);
+        if (!__syncthreads_and(done)) {
+            // The load did not arrive: count it, give the copy in flight one
+            // more bounded wait, and leave this tile unwritten.
+            if (tid == 0 && err) atomicAdd(err, 1);
+            for (uint32_t i = 0; i < kTmaPolls && !mbar_try_wait(&tma_bar, 0); ++i) {
+            }
+            return;
+        }
+    }
     __syncthreads();
 
     const int tx = tid % (TW / PX), ty = tid / (TW / PX);
@@ -129,8 +203,10 @@ template <int TW, int TH, int NK>
 __global__ void __launch_bounds__(DirectTile<TW, TH>::kThreads)
     direct_step_kernel(const float* __restrict__ src, float* __restrict__ dst,
                        const float* __restrict__ weights, const uint32_t* __restrict__ spans,
-                       DirectGeometry g, StepParams p) {
-    direct_tile<TW, TH, NK>(src, dst, weights, spans, g, p, blockIdx.x * TW, blockIdx.y * TH);
+                       DirectGeometry g, StepParams p, const __grid_constant__ CUtensorMap tmap, int use_tma,
+                       int* err) {
+    direct_tile<TW, TH, NK>(src, dst, weights, spans, g, p, blockIdx.x * TW, blockIdx.y * TH,
+                            use_tma ? &tmap : nullptr, err);
 }
 
 // Many worlds in one launch: CTA i computes tile tiles[i] = (world, tile x,
@@ -143,42 +219,54 @@ __global__ void __launch_bounds__(DirectTile<TW, TH>::kThreads)
     const int3 t = tiles[blockIdx.x];
     if (threadIdx.x == 0) w = worlds[t.x];
     __syncthreads();
-    direct_tile<TW, TH, 1>(w.src, w.dst, w.weights, w.spans, w.g, w.p, t.y * TW, t.z * TH);
+    direct_tile<TW, TH, 1>(w.src, w.dst, w.weights, w.spans, w.g, w.p, t.y * TW, t.z * TH, nullptr, nullptr);
 }
 
 template <int TW, int TH, int NK>
 cudaError_t launch_t(const float* src, float* dst, const float* weights, const uint32_t* spans,
-                     const DirectGeometry& g, const StepParams& p, cudaStream_t stream) {
+                     const DirectGeometry& g, const StepParams& p, cudaStream_t stream, const DirectTma* tma,
+                     int buffer) {
     const int TP = TW + 2 * g.xp + 8;
     const size_t smem = sizeof(float) * (size_t(TH + 2 * g.r) * TP + size_t(NK) * g.ksize * g.wp) +
                         sizeof(uint32_t) * NK * g.ksize;
     auto fn = direct_step_kernel<TW, TH, NK>;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;
+    CUtensorMap map;
+    std::memset(&map, 0, sizeof map);
+    const bool on = tma && tma->on && (buffer == 0 || buffer == 1);
+    if (on) std::memcpy(&map, tma->map[buffer], sizeof map);
     dim3 grid((p.width + TW - 1) / TW, (p.height + TH - 1) / TH);
-    fn<<<grid, DirectTile<TW, TH>::kThreads, smem, stream>>>(src, dst, weights, spans, g, p);
+    fn<<<grid, DirectTile<TW, TH>::kThreads, smem, stream>>>(src, dst, weights, spans, g, p, map, on ? 1 : 0,
+                                                             on ? tma->err : nullptr);
     return cudaGetLastError();
 }
 
 template <int TW, int TH>
 cudaError_t launch_nk(int nk, const float* src, float* dst, const float* weights,
                       const uint32_t* spans, const DirectGeometry& g, const StepParams& p,
-                      cudaStream_t s) {
+                      cudaStream_t s, const DirectTma* tma, int buffer) {
     switch (nk) {
-    case 1: return launch_t<TW, TH, 1>(src, dst, weights, spans, g, p, s);
-    case 2: return launch_t<TW, TH, 2>(src, dst, weights, spans, g, p, s);
-    case 3: return launch_t<TW, TH, 3>(src, dst, weights, spans, g, p, s);
-    case 4: return launch_t<TW, TH, 4>(src, dst, weights, spans, g, p, s);
+    case 1: return launch_t<TW, TH, 1>(src, dst, weights, spans, g, p, s, tma, buffer);
+    case 2: return launch_t<TW, TH, 2>(src, dst, weights, spans, g, p, s, tma, buffer);
+    case 3: return launch_t<TW, TH, 3>(src, dst, weights, spans, g, p, s, tma, buffer);
+    case 4: return launch_t<TW, TH, 4>(src, dst, weights, spans, g, p, s, tma, buffer);
     default: return cudaErrorInvalidValue;
     }
+}
+
+void tile_shape(int tile_cfg, int& TW, int& TH) {
+    TW = 64;
+    TH = 16;
+    if (tile_cfg == kDirectTile32x16) { TW = 32; TH = 16; }
+    if (tile_cfg == kDirectTile64x32) { TW = 64; TH = 32; }
 }
 
 }  // namespace
 
 size_t direct_smem_bytes(int tile_cfg, int nk, const DirectGeometry& g) {
-    int TW = 64, TH = 16;
-    if (tile_cfg == kDirectTile32x16) { TW = 32; TH = 16; }
-    if (tile_cfg == kDirectTile64x32) { TW = 64; TH = 32; }
+    int TW, TH;
+    tile_shape(tile_cfg, TW, TH);
     const int TP = TW + 2 * g.xp + 8;
     return sizeof(float) * (size_t(TH + 2 * g.r) * TP + size_t(nk) * g.ksize * g.wp) +
            sizeof(uint32_t) * nk * g.ksize;
@@ -187,13 +275,48 @@ size_t direct_smem_bytes(int tile_cfg, int nk, const DirectGeometry& g) {
 cudaError_t launch_direct_step(int tile_cfg, int nk, const float* src, float* dst,
                                const float* weights, const uint32_t* spans,
                                const DirectGeometry& g, const StepParams& p,
-                               cudaStream_t stream) {
+                               cudaStream_t stream, const DirectTma* tma, int buffer) {
     switch (tile_cfg) {
-    case kDirectTile32x16: return launch_nk<32, 16>(nk, src, dst, weights, spans, g, p, stream);
-    case kDirectTile64x16: return launch_nk<64, 16>(nk, src, dst, weights, spans, g, p, stream);
-    case kDirectTile64x32: return launch_nk<64, 32>(nk, src, dst, weights, spans, g, p, stream);
+    case kDirectTile32x16: return launch_nk<32, 16>(nk, src, dst, weights, spans, g, p, stream, tma, buffer);
+    case kDirectTile64x16: return launch_nk<64, 16>(nk, src, dst, weights, spans, g, p, stream, tma, buffer);
+    case kDirectTile64x32: return launch_nk<64, 32>(nk, src, dst, weights, spans, g, p, stream, tma, buffer);
     default: return cudaErrorInvalidValue;
     }
+}
+
+bool direct_tma_encode(int tile_cfg, const DirectGeometry& g, float* const fields[2], int w, int h, DirectTma& out) {
+    out.on = false;
+    int TW, TH;
+    tile_shape(tile_cfg, TW, TH);
+    const int TP = TW + 2 * g.xp + 8, TR = TH + 2 * g.r;
+    // Row stride a multiple of 16 bytes; the box within the field and within
+    // the 256-element limit per dimension; its rows a multiple of 16 bytes.
+    if (w % 4 != 0 || TP > 256 || TR > 256 || TP > w || TR > h || (TP * 4) % 16 != 0) return false;
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    if (!encode) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !fn) {
+            cudaGetLastError();
+            return false;
+        }
+        encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
+    for (int b = 0; b < 2; ++b) {
+        if (!fields[b] || (reinterpret_cast<uintptr_t>(fields[b]) & 15u) != 0) return false;
+        const cuuint64_t dims[2] = {cuuint64_t(w), cuuint64_t(h)};
+        const cuuint64_t strides[1] = {cuuint64_t(w) * sizeof(float)};
+        const cuuint32_t box[2] = {cuuint32_t(TP), cuuint32_t(TR)};
+        const cuuint32_t estr[2] = {1, 1};
+        const CUresult r = encode(reinterpret_cast<CUtensorMap*>(out.map[b]), CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
+                                  fields[b], dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                  CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) return false;
+    }
+    out.on = true;
+    return true;
 }
 
 cudaError_t launch_direct_worlds(const DirectWorld* worlds, const int3* tiles, int ntiles, int max_r,

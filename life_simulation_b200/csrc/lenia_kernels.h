@@ -36,9 +36,27 @@ struct DirectWorld {
 // tiles[i] = (world, tile x, tile y) of 32x16 output tiles.
 cudaError_t launch_direct_worlds(const DirectWorld* worlds, const int3* tiles, int ntiles, int max_r,
                                  cudaStream_t stream);
+// Halo-tile tensor maps of the direct path: one 2D map per state buffer
+// (cuTensorMapEncodeTiled descriptors, opaque here) whose box is a CTA's halo
+// tile; `err` counts halo loads whose wait ran out (stays 0 on a healthy
+// device).
+struct DirectTma {
+    alignas(64) unsigned char map[2][128];
+    int* err = nullptr;
+    bool on = false;
+};
+// Encodes the maps of fields[0], fields[1] (w x h floats) for the tile shape
+// of `tile_cfg`; false (and on = false) when the size cannot use them: width
+// not a multiple of 4 floats (16-byte row stride), a halo tile wider or taller
+// than the field or than a 256-element box, or no driver entry point.
+bool direct_tma_encode(int tile_cfg, const DirectGeometry& g, float* const fields[2], int w, int h, DirectTma& out);
+// `tma` (or null): interior tiles load their halo with one TMA box from the
+// map of state buffer `buffer` (the one `src` is); edge tiles, whose halo
+// wraps around the torus, keep the wrapped element loads.
 cudaError_t launch_direct_step(int tile_cfg, int nk, const float* src, float* dst,
                                const float* weights, const uint32_t* spans,
-                               const DirectGeometry& g, const StepParams& p, cudaStream_t stream);
+                               const DirectGeometry& g, const StepParams& p, cudaStream_t stream,
+                               const DirectTma* tma = nullptr, int buffer = 0);
 
 // -------------------------------------------------------------------- FFT
 constexpr int kMaxPasses = 8;

@@ -503,6 +503,8 @@ void LeniaModule::release() {
     };
     rel(field_[0]);
     rel(field_[1]);
+    rel(d_tma_err_);
+    direct_tma_ = DirectTma();
     rel(d_weights_);
     rel(d_spans_);
     rel(d_org_);
@@ -772,6 +774,58 @@ int LeniaModule::buildDirectTables() {
     else if (tiles(64, 16) >= 2 * sms) direct_tile_ = kDirectTile64x16;
     else direct_tile_ = kDirectTile32x16;
     if (direct_smem_bytes(direct_tile_, direct_nk_, dgeo_) > 220 * 1024) direct_tile_ = kDirectTile32x16;
+    // Halo tiles by TMA where the size allows it (interior tiles only).
+    // LENIA_DIRECT_TMA in the environment at setup: 0 keeps element loads,
+    // 1 uses TMA wherever the size allows; unset, the faster one here.
+    const char* tma_env = std::getenv("LENIA_DIRECT_TMA");
+    const bool tma_off = tma_env && tma_env[0] == '0' && tma_env[1] == '\0';
+    const bool tma_forced = tma_env && tma_env[0] == '1' && tma_env[1] == '\0';
+    if (!tma_off && direct_tma_encode(direct_tile_, dgeo_, field_, int(w_), int(h_), direct_tma_)) {
+        if ((e = dev_alloc(&d_tma_err_, 1, device_bytes_)) != cudaSuccess) return cudaFail(e, "cudaMalloc flags");
+        cudaMemset(d_tma_err_, 0, sizeof(int));
+        direct_tma_.err = d_tma_err_;
+    }
+    if (direct_tma_.on && !tma_forced) {
+        // One bulk copy per CTA wins on small fields and loses to the
+        // element loads of many CTAs on large ones: keep whichever is faster
+        // here (a few steps each on the context's own buffers).
+        StepParams p{};
+        p.width = w_;
+        p.height = h_;
+        p.num_kernels = uint32_t(direct_nk_);
+        for (int k = 0; k < 4; ++k) p.sigma[k] = 1.0f;
+        cudaEvent_t a = takeEvent(), b = takeEvent();
+        float best[2] = {1e30f, 1e30f};
+        for (int rep = 0; rep < 3; ++rep)
+            for (int v = 0; v < 2; ++v) {
+                cudaEventRecord(a, stream_);
+                for (int i = 0; i < 3; ++i)
+                    launch_direct_step(direct_tile_, direct_nk_, field_[0], field_[1], d_weights_, d_spans_, dgeo_, p,
+                                       stream_, v ? &direct_tma_ : nullptr, 0);
+                cudaEventRecord(b, stream_);
+                cudaEventSynchronize(b);
+                float ms = 0.0f;
+                if (cudaEventElapsedTime(&ms, a, b) == cudaSuccess && rep > 0) best[v] = std::min(best[v], ms);
+            }
+        event_pool_.push_back(a);
+        event_pool_.push_back(b);
+        cudaMemsetAsync(field_[1], 0, sizeof(float) * w_ * h_, stream_);
+        if ((e = cudaGetLastError()) != cudaSuccess) return cudaFail(e, "direct staging choice");
+        if (!(best[1] < best[0])) direct_tma_.on = false;
+    }
+    return LENIA_OK;
+}
+
+int LeniaModule::checkDeviceFlags() {
+    if (!d_tma_err_) return LENIA_OK;
+    int n = 0;
+    const cudaError_t e = cudaMemcpy(&n, d_tma_err_, sizeof n, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cudaFail(e, "read device flags");
+    if (n != 0) {
+        cudaMemset(d_tma_err_, 0, sizeof(int));
+        return fail(LENIA_ERR_CUDA, "direct path: " + std::to_string(n) +
+                                        " halo tile load(s) did not arrive in time; those tiles were not written");
+    }
     return LENIA_OK;
 }
 
@@ -1180,7 +1234,8 @@ int LeniaModule::stepImpl(const lenia_frame_params& fp, uint32_t substeps, cudaS
             spectrum_valid_ = true;
         } else {
             e = launch(LENIA_PHASE_DIRECT, s, [&] {
-                return launch_direct_step(direct_tile_, direct_nk_, src, dst, d_weights_, d_spans_, dgeo_, p, s);
+                return launch_direct_step(direct_tile_, direct_nk_, src, dst, d_weights_, d_spans_, dgeo_, p, s,
+                                          &direct_tma_, cur_);
             });
             if (e != cudaSuccess) return cudaFail(e, "direct step");
         }
@@ -1199,6 +1254,7 @@ void LeniaModule::info(lenia_info* o) const {
     o->use_stamp_init = use_stamp_ ? 1u : 0u;
     o->device_bytes = device_bytes_;
     o->fft_precision = tc_precision_;
+    o->direct_tma = (!use_fft_ && direct_tma_.on) ? 1u : 0u;
     if (use_fft_) {
         for (int i = 0; i < fgeo_.row.npass && i < 8; ++i) o->fft_radix_row[i] = uint32_t(fgeo_.row.radix[i]);
         for (int i = 0; i < fgeo_.col.npass && i < 8; ++i) o->fft_radix_col[i] = uint32_t(fgeo_.col.radix[i]);

@@ -134,6 +134,10 @@ public:
 
     // Per-launch event timing (GPUTimer's role, LifeCore/Metal/GPUTimer.h).
     void setProfiling(bool on);
+    // Device-side failures recorded by the kernels (read after a sync):
+    // LENIA_OK, or an error with its message.
+    int checkDeviceFlags();
+    bool directTma() const { return direct_tma_.on; }
     int readProfile(lenia_profile_data* out);
 
 private:
@@ -185,6 +189,8 @@ private:
 
     // Device resources.
     float* field_[2] = {nullptr, nullptr};
+    DirectTma direct_tma_;          // halo-tile tensor maps of field_[0], field_[1]
+    int* d_tma_err_ = nullptr;      // halo loads whose wait ran out
     float* d_weights_ = nullptr;
     uint32_t* d_spans_ = nullptr;
     float* d_org_ = nullptr;

@@ -300,3 +300,31 @@ def test_zero_radius_and_tiny_fields():
         init = np.random.default_rng(w).random((h, w)).astype(np.float32)
         for g, o in run_pair(p, w, h, init, 3, "ref32"):
             assert np.abs(g - o).max() < 2e-5, (p, w, h)
+
+
+@pytest.mark.parametrize("w,h,radius", [(256, 256, 13), (512, 320, 32), (200, 120, 7)])
+def test_direct_tma_halo_tiles_equal_element_loads(monkeypatch, w, h, radius):
+    """The direct path's interior halo tiles arrive by one TMA box load each
+    (edge tiles, whose halo wraps around the torus, by element loads): the
+    field is bit-identical to staging every tile by element loads."""
+    params = {"radius": radius, "noiseAmount": 0.05, "muJitter": 0.2}
+    init = wl.patches(w, h, 8, 40, seed=9)
+    out = []
+    for env in ("1", "0"):
+        monkeypatch.setenv("LENIA_DIRECT_TMA", env)
+        m = lb.LeniaModule(params, w, h)
+        assert m.info()["direct_tma"] == (env == "1")
+        m.reset(5)
+        m.upload(init)
+        for f in range(4):
+            m.encode(f, 2)
+        m.sync()
+        out.append(m.field())
+        m.close()
+    np.testing.assert_array_equal(out[0], out[1])
+
+
+def test_direct_tma_off_for_unaligned_widths():
+    m = lb.LeniaModule({"radius": 5}, 37, 23)  # row stride not a multiple of 16 bytes
+    assert m.info()["direct_tma"] is False
+    m.close()
