@@ -35,6 +35,9 @@ pixels x steps; ``value`` is whole-job Mpixel-steps/s.
   (a radix-16 stage as a real 32x32 GEMM: 128 FLOP per point, x3 hi/lo).
 * library_fft_baseline: the same step from torch.fft (cuFFT) and torch ops
   in one CUDA graph, same flush protocol: a library comparator.
+* published_config: 1024x512, 3 kernels R=24 -- the one FFT configuration
+  the reference publishes a time for (Apple M5 Max, README.md:47-48) --
+  timed the same way, beside that published figure.
 * --impl reference: that CPU reference alone, as the reference arm.
 """
 from __future__ import annotations
@@ -190,6 +193,45 @@ def cpu_baseline_port(params, w, h, init, seconds):
             break
     return {"value": w * h * steps / el / 1e6, "unit": UNIT, "cores": 1, "kind": "port",
             "sample": f"full {w}x{h} field, {steps} substeps in {el:.1f} s (FP64 oracle)"}
+
+
+def published_config_bench(steps: int = 100, warmup: int = 5) -> dict:
+    """The one FFT configuration the reference publishes a number for:
+    1024x512, 3 kernels, R=24 (README.md:47-48, 1.13 ms per frame on an Apple
+    M5 Max through Metal, one substep per frame). Same timing as the value
+    region (L2 flushed before each step, CUDA events, launch shapes as the
+    setup autotuner picked them)."""
+    import torch
+
+    import life_simulation_b200 as lb
+    from life_simulation_b200 import workloads as wl
+
+    params, w, h, init = wl.workload("fft3_1024x512")
+    m = lb.LeniaModule(params, w, h)
+    m.reset(2)
+    m.upload(init)
+    stream = torch.cuda.Stream()
+    sh = stream.cuda_stream
+    fp = m.frame_params(0)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    evs = []
+    with torch.cuda.stream(stream):
+        for i in range(warmup + steps):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            m.step(fp, 1, sh)
+            b.record(stream)
+            if i >= warmup:
+                evs.append((a, b))
+    torch.cuda.synchronize()
+    ms = float(np.mean([a.elapsed_time(b) for a, b in evs]))
+    m.close()
+    ref_ms = 1.13
+    return {"workload": "fft3_1024x512: 1024x512, 3 kernels R=24 (the reference's published FFT configuration)",
+            "ms_per_step": ms, "value": w * h / (ms / 1e3) / 1e6, "unit": UNIT,
+            "reference_published": {"ms_per_frame": ref_ms, "value": w * h / (ref_ms / 1e3) / 1e6,
+                                    "hardware": "Apple M5 Max (Metal), README.md:47-48; not reproducible here"}}
 
 
 def library_fft_baseline(params, w, h, init, steps: int = 50, warmup: int = 5) -> dict:
@@ -502,6 +544,8 @@ def run_b200(args):
         line["adjoint"] = adjoint_bench(args.adjoint_reps)
     if rank == 0 and world == 1 and not args.no_library_baseline:
         line["library_fft_baseline"] = library_fft_baseline(params, w, h, init)
+    if rank == 0 and world == 1 and args.workload == WORKLOAD:
+        line["published_config"] = published_config_bench()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_baseline(params, w, h, init, args.cpu_seconds)
