@@ -549,7 +549,7 @@ def run_b200(args):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_baseline(params, w, h, init, args.cpu_seconds)
-        except Exception as e:  # the checker is optional; the GPU number stands
+        except Exception as e:  # the oracle is optional here; the GPU number stands
             line["cpu_baseline"] = {"value": None, "error": str(e)}
     if rank == 0:
         print(json.dumps(line))
@@ -627,7 +627,7 @@ def run_adjoint(args):
 
 
 def run_tc(args):
-    """the column DFT stages on the CUDA cores (FP32) and
+    """4096x4096, 3 kernels R=32: the column DFT stages on the CUDA cores (FP32) and
     on the tensor cores (FP16 / BF16 hi/lo, FP32 accumulation)."""
     import torch
 
@@ -694,7 +694,7 @@ def run_tc(args):
 
 
 def run_sweep(args):
-    """512 worlds of mixed sizes, 240 substeps with the
+    """The 512-world sweep: 512 worlds of mixed sizes, 240 substeps with the
     activity readback every 60, batched (one graph per 60 substeps) against
     the plain form (one context per world, worlds stepped one at a time)."""
     import torch

@@ -6,7 +6,7 @@
 namespace lenia {
 
 constexpr int kMaxKernels = 4;   // Lenia.cpp:225-230 caps "kernels" at 4
-constexpr int kMaxRadius = 32;   // direct path radius limit of this build
+constexpr int kMaxRadius = 32;   // direct path radius limit of this library
 constexpr int kMaxBetas = 8;     // kernel shells per kernel
 
 // Everything one substep's growth epilogue needs. It merges the reference's

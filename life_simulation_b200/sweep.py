@@ -2,7 +2,7 @@
 
 The reference explores a scene's parameters one variant at a time: each
 variant is a copy of the scene with some module params overridden, run in its
-own SceneRunner for a number of frames, and judged by the activity of its
+own SceneRunner for a number of frames, and rated by the activity of its
 colour layer (Apps/LifePresetLab/main.cpp). This module keeps that
 vocabulary -- the sweep file, the variant enumeration, the overrides, the
 luma activity and the "alive" rule -- and runs all variants at once as the

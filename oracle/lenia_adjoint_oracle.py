@@ -1,7 +1,8 @@
 """FP64 oracle of the spectral Lenia step's adjoint (test infrastructure).
 
 Only tests, the smoke entry and the benchmark's CPU baseline use this module,
-as the checker of the CUDA adjoint; the product never calls it.
+as the reference the CUDA adjoint is compared against; the product never
+calls it.
 
 The reference has no adjoint. The forward it differentiates is the reference's
 multi-kernel spectral step without noise, mu jitter or injection:

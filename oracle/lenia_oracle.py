@@ -1,6 +1,6 @@
 """CPU oracle for the Lenia field update -- TEST INFRASTRUCTURE ONLY.
 
-This module is the checker the CUDA path is compared against. Only tests/,
+This module is the oracle the CUDA path is compared against. Only tests/,
 ``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py`` may import
 it; the product never does.
 

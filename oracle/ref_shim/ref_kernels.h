@@ -10,7 +10,7 @@
 // Runs pipeline `fn` over a w x h grid. tex[i] is the image bound at
 // [[texture(i)]], bytes[i]/nbytes[i] the uniform block bound at [[buffer(i)]].
 // Only grid rows [y0, y1) run (0, ~0u: all). Returns false for a pipeline
-// name this build does not know.
+// name this shim does not know.
 bool ref_dispatch(const std::string& fn, metal::CpuImage* const* tex, const void* const* bytes,
                   const size_t* nbytes, uint32_t w, uint32_t h, uint32_t y0, uint32_t y1);
 

@@ -126,7 +126,7 @@ def local_errors(params, w, h, init, steps):
 
 
 def test_direct_single_256_100_steps_vs_fp64():
-    # Per-step error over the whole 100-step run ...
+    # Per-step error over the whole 100-step run of the 256x256 direct workload ...
     params, w, h, init = wl.workload("single_256")
     errs = local_errors(params, w, h, init, 100)
     assert errs.max() <= 1e-5, errs.max()

@@ -1,7 +1,7 @@
 """Column DFT stages on the tensor cores (fftPrecision "bf16x3" / "fp16x3",
 split-precision operands with FP32 accumulation): per-step error against the
 FP64 oracle beside the FP32 CUDA-core path, at 512x256 and at 4096x4096
-(BASELINE config 4's size), plus the size fallback."""
+(3 kernels, R=32), plus the size fallback."""
 import numpy as np
 import pytest
 
@@ -67,7 +67,7 @@ def test_tensor_core_columns_per_step_vs_fp64(prec):
 
 
 def test_tensor_core_columns_4096():
-    """BASELINE config 4's field: 4096x4096, 3 kernels R=32."""
+    """The 4096x4096 field with 3 kernels of radius 32."""
     w = h = 4096
     init = wl.patches(w, h, 40, 256, seed=2)
     for prec in ("fp32", "fp16x3", "bf16x3"):
