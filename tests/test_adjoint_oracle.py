@@ -119,7 +119,7 @@ def test_sharded_parameter_gradients_allreduce_to_full_batch():
     assert [list(shard_worlds(5, 2, r)) for r in range(2)] == [[0, 1, 2], [3, 4]]
     assert sum(len(shard_worlds(32, 3, r)) for r in range(3)) == 32
     world_size = 2
-    mgr = mp.Manager()
+    mgr = mp.get_context("spawn").Manager()
     out = mgr.dict()
     mp.spawn(_rank_main, args=(world_size, _free_port(), out), nprocs=world_size, join=True)
     p, a0, target = small_case(0, batch=5, w=24, h=24)
