@@ -194,12 +194,20 @@ def scene_world(scene: dict, module: str):
 
 
 def run_sweep(scene: dict, sweep, frames: int = 240, substeps: int = 1, module: str = "lenia0",
-              policy: int = BATCH_AUTO) -> dict:
+              policy: int = BATCH_AUTO, rank: int = 0, world_size: int = 1, group=None) -> dict:
     """Every variant of `sweep` on `scene`, run together for `frames` frames
     of `substeps` substeps; activity measured on the last frame (the lab's
     default thumbnail). Returns {"mode", "frames", "variants": [{"id", "seed",
     "overrides", "activity": {"meanLuma", "stddevLuma", "alive"}}],
-    "aliveCount"}."""
+    "aliveCount"}.
+
+    With world_size > 1 (one process per GPU, torch.distributed initialised)
+    every rank runs its cost-balanced share of the variants
+    (life_simulation_b200.shard.partition) as its own batch and the per-
+    variant records are gathered afterwards: every rank returns the same
+    result as one GPU would."""
+    from .shard import gather_records, partition, world_cost
+
     cfg = sweep if isinstance(sweep, SweepConfig) else load_sweep(sweep)
     if frames < 1:
         raise SweepError("frames must be >= 1")
@@ -215,18 +223,28 @@ def run_sweep(scene: dict, sweep, frames: int = 240, substeps: int = 1, module: 
             cmap = cm
         elif bytes(cm) != bytes(cmap):
             raise SweepError("all variants must share one colour map")
-    batch = LeniaBatch(worlds, policy)
-    for i, (seed, cov, scale) in enumerate(inits):
-        batch.init_noise(i, seed, cov, scale)
-    batch.step(frames * max(1, substeps))
-    mean, std = batch.activity(cmap)
-    paths = [batch.path(i) for i in range(len(variants))]
-    batch.close()
-    out = []
-    for i, v in enumerate(variants):
-        out.append({"id": v.id, "seed": v.seed, "overrides": {t: val for t, val in v.overrides},
-                    "activity": {"meanLuma": float(mean[i]), "stddevLuma": float(std[i]),
-                                 "alive": is_alive(float(mean[i]), float(std[i]))},
-                    "path": "fft" if paths[i] == 1 else "direct"})
+    mine = list(range(len(variants)))
+    if world_size > 1:
+        costs = [world_cost(w.width, w.height, w.radius) for w in worlds]
+        mine = partition(costs, world_size)[rank]
+    records = []
+    if mine:
+        batch = LeniaBatch([worlds[i] for i in mine], policy)
+        for j, i in enumerate(mine):
+            batch.init_noise(j, *inits[i])
+        batch.step(frames * max(1, substeps))
+        mean, std = batch.activity(cmap)
+        paths = [batch.path(j) for j in range(len(mine))]
+        batch.close()
+        for j, i in enumerate(mine):
+            v = variants[i]
+            records.append({"world": i, "id": v.id, "seed": v.seed,
+                            "overrides": {t: val for t, val in v.overrides},
+                            "activity": {"meanLuma": float(mean[j]), "stddevLuma": float(std[j]),
+                                         "alive": is_alive(float(mean[j]), float(std[j]))},
+                            "path": "fft" if paths[j] == 1 else "direct"})
+    if world_size > 1:
+        records = gather_records(records, group)
+    out = [{k: r[k] for k in ("id", "seed", "overrides", "activity", "path")} for r in records]
     return {"mode": cfg.mode, "frames": frames, "substeps": substeps, "variants": out,
             "aliveCount": sum(1 for e in out if e["activity"]["alive"])}

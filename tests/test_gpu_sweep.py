@@ -66,3 +66,44 @@ def test_sweep_matches_one_variant_at_a_time():
         assert act["alive"] == is_alive(mean, std) or min(abs(mean - 0.01), abs(mean - 0.7), abs(std - 0.02)) < 1e-4
         alive += act["alive"]
     assert res["aliveCount"] == alive
+
+
+def _sharded_rank(rank, world_size, port, out):
+    import os
+
+    import torch.distributed as dist
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world_size)
+    try:
+        out[rank] = run_sweep(SCENE, SWEEP, frames=8, policy=lb.BATCH_DIRECT, rank=rank, world_size=world_size)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_sweep_sharded_over_two_processes_equals_one():
+    """Two ranks (here both on the one GPU, each with its own independent
+    batch; only the per-variant records cross, on the host) give the same
+    result as the whole sweep in one process."""
+    import socket
+
+    import torch.multiprocessing as mp
+
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    ctx = mp.get_context("spawn")
+    out = ctx.Manager().dict()
+    mp.spawn(_sharded_rank, args=(2, port, out), nprocs=2, join=True)
+    whole = run_sweep(SCENE, SWEEP, frames=8, policy=lb.BATCH_DIRECT)
+    for r in range(2):
+        got = out[r]
+        assert [v["id"] for v in got["variants"]] == [v["id"] for v in whole["variants"]]
+        for a, b in zip(got["variants"], whole["variants"]):
+            # Same fields; the FP64 luma sums may add in another order
+            # (atomics over a differently sized grid).
+            for k in ("meanLuma", "stddevLuma"):
+                assert a["activity"][k] == pytest.approx(b["activity"][k], rel=1e-12, abs=1e-15), (a["id"], k)
+            assert a["activity"]["alive"] == b["activity"]["alive"]
+        assert got["aliveCount"] == whole["aliveCount"]
