@@ -400,19 +400,22 @@ __global__ void __launch_bounds__(ColK<PF, B>::T)
             ok[it] = q < B * NRL && bi[it] < cols;
         }
         // Kernel spectrum values of this thread's elements, one kernel
-        // ahead (kv2: the Nyquist column's value, for the packed column 0).
-        float kv[ITL][RL], kv2[ITL][RL];
+        // ahead (last passes of radix <= 8 only, as in the forward pass).
+        constexpr bool kAhead = RL <= 8;
+        float kv[ITL][kAhead ? RL : 1], kv2[ITL][kAhead ? RL : 1];  // kv2: Nyquist column (packed column 0)
         const auto fetch_k = [&](int kk) {
-            const float* kh = a.khat + size_t(kk) * (M + 1) * Hh;
+            if constexpr (kAhead) {
+                const float* kh = a.khat + size_t(kk) * (M + 1) * Hh;
 #pragma unroll
-            for (int it = 0; it < ITL; ++it) {
-                const int kx = k0 + bi[it];
+                for (int it = 0; it < ITL; ++it) {
+                    const int kx = k0 + bi[it];
 #pragma unroll
-                for (int t = 0; t < RL; ++t) {
-                    const int ky = jj[it] + t * NRL;
-                    const int kyr = min(ky, H - ky);
-                    kv[it][t] = ok[it] ? __ldg(kh + size_t(kx) * Hh + kyr) : 0.0f;
-                    kv2[it][t] = (ok[it] && kx == 0) ? __ldg(kh + size_t(M) * Hh + kyr) : 0.0f;
+                    for (int t = 0; t < RL; ++t) {
+                        const int ky = jj[it] + t * NRL;
+                        const int kyr = min(ky, H - ky);
+                        kv[it][t] = ok[it] ? __ldg(kh + size_t(kx) * Hh + kyr) : 0.0f;
+                        kv2[it][t] = (ok[it] && kx == 0) ? __ldg(kh + size_t(M) * Hh + kyr) : 0.0f;
+                    }
                 }
             }
         };
@@ -448,16 +451,26 @@ __global__ void __launch_bounds__(ColK<PF, B>::T)
             for (int it = 0; it < ITL; ++it) {
                 if (!ok[it]) continue;
                 const int kx = k0 + bi[it];
+                const float* kh = a.khat + size_t(kk) * (M + 1) * Hh;
 #pragma unroll
                 for (int t = 0; t < RL; ++t) {
                     const int ky = jj[it] + t * NRL;
+                    const int kyr = min(ky, H - ky);
+                    float kval, knyq;
+                    if constexpr (kAhead) {
+                        kval = kv[it][t];
+                        knyq = kv2[it][t];
+                    } else {
+                        kval = __ldg(kh + size_t(kx) * Hh + kyr);
+                        knyq = kx == 0 ? __ldg(kh + size_t(M) * Hh + kyr) : 0.0f;
+                    }
                     float2 D;
                     if (kx == 0) {
-                        const float P = kv[it][t], Qn = kv2[it][t];
+                        const float P = kval, Qn = knyq;
                         const float2 Cm = cconj(c0q[ky == 0 ? 0 : H - ky]);
                         D = cadd(cscale(Q[it][t], 0.5f * (P + Qn)), cscale(Cm, 0.5f * (P - Qn)));
                     } else {
-                        D = cscale(Q[it][t], kv[it][t]);
+                        D = cscale(Q[it][t], kval);
                     }
                     G[it][t] = kk == 0 ? D : cadd(G[it][t], D);
                 }

@@ -484,21 +484,37 @@ int lenia_batch_create(const lenia_world* worlds, uint32_t n, uint32_t policy, l
             }
             return best;
         };
-        std::vector<int> dcand;
-        double taps = 0.0;
+        // Cost per tap of the batched direct launch over every candidate.
+        // That launch sizes its halo tile for the largest radius it holds,
+        // which overstates the cost for small radii; so candidates are also
+        // timed in radius bands, each with its own halo, and a band with
+        // enough work (>= 1e8 pixel-taps, so the launch itself is amortised)
+        // uses its own figure.
+        const auto band = [&](uint32_t i) { return worlds[i].radius <= 12u ? 0 : worlds[i].radius <= 20u ? 1 : 2; };
+        std::vector<int> dall, dcand[3];
+        double taps_all = 0.0, taps[3] = {0.0, 0.0, 0.0};
         for (uint32_t i = 0; i < n; ++i)
             if (can_direct[i] && can_fft[i]) {
-                dcand.push_back(int(i));
-                taps += double(worlds[i].width) * worlds[i].height * nnz[i];
+                const double t = double(worlds[i].width) * worlds[i].height * nnz[i];
+                dall.push_back(int(i));
+                dcand[band(i)].push_back(int(i));
+                taps_all += t;
+                taps[band(i)] += t;
             }
-        double cost_tap = 0.0;
-        if (!dcand.empty()) {
+        const auto time_direct = [&](const std::vector<int>& ids, double t, double& out) {
             DirectWorld* dt[2] = {nullptr, nullptr};
             int3* tl = nullptr;
             int nt = 0, mr = 0;
-            if (build_direct(dcand, dt, &tl, &nt, &mr) < 0) return LENIA_ERR_CUDA;
+            if (build_direct(ids, dt, &tl, &nt, &mr) < 0) return false;
             const float ms = time_ms([&] { return launch_direct_worlds(dt[0], tl, nt, mr, b.stream); });
-            cost_tap = double(ms) / taps;
+            out = double(ms) / t;
+            return true;
+        };
+        double cost_all = 0.0, cost_tap[3] = {0.0, 0.0, 0.0};
+        if (!dall.empty() && !time_direct(dall, taps_all, cost_all)) return LENIA_ERR_CUDA;
+        for (int bd = 0; bd < 3; ++bd) {
+            cost_tap[bd] = cost_all;
+            if (taps[bd] >= 1e8 && !time_direct(dcand[bd], taps[bd], cost_tap[bd])) return LENIA_ERR_CUDA;
         }
         std::vector<double> cost_px(b.classes.size(), 0.0);
         for (size_t ci = 0; ci < b.classes.size(); ++ci) {
@@ -518,7 +534,7 @@ int lenia_batch_create(const lenia_world* worlds, uint32_t n, uint32_t policy, l
         cudaEventDestroy(eb);
         for (uint32_t i = 0; i < n; ++i)
             if (can_direct[i] && can_fft[i])
-                b.path[i] = (cost_tap * nnz[i] <= cost_px[size_t(cls[i])]) ? LENIA_CONV_DIRECT : LENIA_CONV_FFT;
+                b.path[i] = (cost_tap[band(i)] * nnz[i] <= cost_px[size_t(cls[i])]) ? LENIA_CONV_DIRECT : LENIA_CONV_FFT;
         cudaMemsetAsync(b.fields, 0, total * sizeof(float), b.stream);
     }
 

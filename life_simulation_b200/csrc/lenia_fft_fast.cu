@@ -120,20 +120,24 @@ __global__ void __launch_bounds__(ColK<PF, B>::T)
         }
         // Kernel spectrum values of this thread's last-pass elements, one
         // kernel ahead: kernel 0's are in flight during the forward
-        // transform, kernel k+1's during kernel k's inverse. kv2 is the
-        // Nyquist column's value, used by the packed column 0 only.
-        float kv[K::ITL][RL], kv2[K::ITL][RL];
+        // transform, kernel k+1's during kernel k's inverse. Only for last
+        // passes of radix <= 8: with 16 values per item the extra registers
+        // cost more occupancy than the hidden latency gains.
+        constexpr bool kAhead = RL <= 8;
+        float kv[K::ITL][kAhead ? RL : 1], kv2[K::ITL][kAhead ? RL : 1];  // kv2: Nyquist column (packed column 0)
         const auto fetch_k = [&](int kk) {
-            const float* kh = khat + size_t(kk) * (M + 1) * Hh;
+            if constexpr (kAhead) {
+                const float* kh = khat + size_t(kk) * (M + 1) * Hh;
 #pragma unroll
-            for (int it = 0; it < K::ITL; ++it) {
-                const int kx = k0 + bi[it];
+                for (int it = 0; it < K::ITL; ++it) {
+                    const int kx = k0 + bi[it];
 #pragma unroll
-                for (int t = 0; t < RL; ++t) {
-                    const int ky = jj[it] + t * NRL;
-                    const int kyr = min(ky, H - ky);
-                    kv[it][t] = ok[it] ? __ldg(kh + size_t(kx) * Hh + kyr) : 0.0f;
-                    kv2[it][t] = (ok[it] && kx == 0) ? __ldg(kh + size_t(M) * Hh + kyr) : 0.0f;
+                    for (int t = 0; t < RL; ++t) {
+                        const int ky = jj[it] + t * NRL;
+                        const int kyr = min(ky, H - ky);
+                        kv[it][t] = ok[it] ? __ldg(kh + size_t(kx) * Hh + kyr) : 0.0f;
+                        kv2[it][t] = (ok[it] && kx == 0) ? __ldg(kh + size_t(M) * Hh + kyr) : 0.0f;
+                    }
                 }
             }
         };
@@ -177,15 +181,25 @@ __global__ void __launch_bounds__(ColK<PF, B>::T)
                 if (!ok[it]) continue;
                 const int kx = k0 + bi[it];
                 float2 D[RL];
+                const float* kh = khat + size_t(kk) * (M + 1) * Hh;
 #pragma unroll
                 for (int t = 0; t < RL; ++t) {
                     const int ky = jj[it] + t * NRL;
+                    const int kyr = min(ky, H - ky);
+                    float kval, knyq;
+                    if constexpr (kAhead) {
+                        kval = kv[it][t];
+                        knyq = kv2[it][t];
+                    } else {
+                        kval = __ldg(kh + size_t(kx) * Hh + kyr);
+                        knyq = kx == 0 ? __ldg(kh + size_t(M) * Hh + kyr) : 0.0f;
+                    }
                     if (kx == 0) {
-                        const float P = kv[it][t], Q = kv2[it][t];
+                        const float P = kval, Q = knyq;
                         const float2 Cm = cconj(c0[ky == 0 ? 0 : H - ky]);
                         D[t] = cadd(cscale(C[it][t], 0.5f * (P + Q)), cscale(Cm, 0.5f * (P - Q)));
                     } else {
-                        D[t] = cscale(C[it][t], kv[it][t]);
+                        D[t] = cscale(C[it][t], kval);
                     }
                 }
                 Dft<RL, true>::run(D);
@@ -233,7 +247,7 @@ static __device__ __noinline__ void palette_pair(const ColorMapParams& cm, float
 // (one staging buffer, which doubles as the second work buffer) each item is
 // staged and waited for in turn: less shared memory per CTA, which wins
 // where shared memory limits the resident CTAs (long rows).
-template <class PI, int RB, bool PIPE>
+template <class PI, int RB, bool PIPE, bool CM>
 __global__ void __launch_bounds__(RowK<PI, RB>::T, (512 / RowK<PI, RB>::T > 1 ? 512 / RowK<PI, RB>::T : 1))
     row_fast_kernel(SpectralWorld w0, const SpectralWorld* __restrict__ worlds,
                     const float2* __restrict__ twr_g, const float2* __restrict__ twi_g,
@@ -377,7 +391,7 @@ __global__ void __launch_bounds__(RowK<PI, RB>::T, (512 / RowK<PI, RB>::T > 1 ? 
                                 growth_finish_lean(p, a.y, acc[it][t][1], acc[it][t][1], uint32_t(2 * n + 1),
                                                    uint32_t(gy)));
                 *reinterpret_cast<float2*>(A_out + size_t(gy) * W + 2 * n) = r;
-                if (sw.rgba) palette_pair(sw.cm, r, sw.rgba + size_t(gy) * W + 2 * n);
+                if constexpr (CM) palette_pair(sw.cm, r, sw.rgba + size_t(gy) * W + 2 * n);
                 za[it][t] = r;
             }
         }
@@ -428,11 +442,11 @@ cudaError_t launch_col_t(const SpectralWorld& w0, const SpectralWorld* worlds, i
     return launch_chained(fn, world_grid(per, (M + B - 1) / B, n), K::T, smem, s, w0, worlds, t.col_twf, t.col_twi);
 }
 
-template <class PI, int RB, bool PIPE>
+template <class PI, int RB, bool PIPE, bool CM>
 cudaError_t launch_row_t(const SpectralWorld& w0, const SpectralWorld* worlds, int n, int H,
                          const float2* tw_r2c, const FastTables& t, cudaStream_t s) {
     using K = RowK<PI, RB>;
-    auto fn = row_fast_kernel<PI, RB, PIPE>;
+    auto fn = row_fast_kernel<PI, RB, PIPE, CM>;
     const size_t smem = K::smem(PIPE ? 3 : 2);
     if (smem > 227 * 1024) return cudaErrorInvalidConfiguration;
     cudaError_t e = prepare(fn, smem);
@@ -511,25 +525,35 @@ cudaError_t col_dispatch(int H, int M, int batch, const SpectralWorld& w0, const
     }
 }
 
-cudaError_t row_dispatch(int H, int M, int batch, const SpectralWorld& w0, const SpectralWorld* worlds, int n,
-                         const float2* tw_r2c, const FastTables& t, cudaStream_t s) {
+// CM: the variant that also writes the colour layer (w0.rgba); the other
+// launches use the one compiled without that store, which would otherwise
+// cost every row pass a few per cent.
+template <bool CM>
+cudaError_t row_dispatch_t(int H, int M, int batch, const SpectralWorld& w0, const SpectralWorld* worlds, int n,
+                           const float2* tw_r2c, const FastTables& t, cudaStream_t s) {
     const int rb = batch & ~kRowPipelined;
     const bool pipe = (batch & kRowPipelined) != 0;
     switch (M) {
-#define X(m, ...)                                                                                  \
-    case m:                                                                                        \
-        if (pipe) {                                                                                \
-            if (rb == 4) return launch_row_t<__VA_ARGS__, 4, true>(w0, worlds, n, H, tw_r2c, t, s); \
-            if (rb == 2) return launch_row_t<__VA_ARGS__, 2, true>(w0, worlds, n, H, tw_r2c, t, s); \
-            return launch_row_t<__VA_ARGS__, 1, true>(w0, worlds, n, H, tw_r2c, t, s);              \
-        }                                                                                          \
-        if (rb == 4) return launch_row_t<__VA_ARGS__, 4, false>(w0, worlds, n, H, tw_r2c, t, s);    \
-        if (rb == 2) return launch_row_t<__VA_ARGS__, 2, false>(w0, worlds, n, H, tw_r2c, t, s);    \
-        return launch_row_t<__VA_ARGS__, 1, false>(w0, worlds, n, H, tw_r2c, t, s);
+#define X(m, ...)                                                                                      \
+    case m:                                                                                            \
+        if (pipe) {                                                                                    \
+            if (rb == 4) return launch_row_t<__VA_ARGS__, 4, true, CM>(w0, worlds, n, H, tw_r2c, t, s); \
+            if (rb == 2) return launch_row_t<__VA_ARGS__, 2, true, CM>(w0, worlds, n, H, tw_r2c, t, s); \
+            return launch_row_t<__VA_ARGS__, 1, true, CM>(w0, worlds, n, H, tw_r2c, t, s);              \
+        }                                                                                              \
+        if (rb == 4) return launch_row_t<__VA_ARGS__, 4, false, CM>(w0, worlds, n, H, tw_r2c, t, s);    \
+        if (rb == 2) return launch_row_t<__VA_ARGS__, 2, false, CM>(w0, worlds, n, H, tw_r2c, t, s);    \
+        return launch_row_t<__VA_ARGS__, 1, false, CM>(w0, worlds, n, H, tw_r2c, t, s);
         LENIA_ROW_PLANS(X)
 #undef X
     default: return cudaErrorNotSupported;
     }
+}
+
+cudaError_t row_dispatch(int H, int M, int batch, const SpectralWorld& w0, const SpectralWorld* worlds, int n,
+                         const float2* tw_r2c, const FastTables& t, cudaStream_t s) {
+    if (w0.rgba && !worlds) return row_dispatch_t<true>(H, M, batch, w0, worlds, n, tw_r2c, t, s);
+    return row_dispatch_t<false>(H, M, batch, w0, worlds, n, tw_r2c, t, s);
 }
 
 template <class PF, int B>
