@@ -62,7 +62,7 @@ WORKLOAD = "fft3_1080p"
 FALLBACK_HBM_GBS = 6650.0
 # dram__bytes_read.sum + dram__bytes_write.sum per launch from one ncu
 # capture of the default workload (profiles/lenia_fft_step_1080p_k3.md).
-NCU_TRAFFIC_BYTES = {"row_growth": 33_261_056 + 26_112, "column": 14_575_616 + 0}
+NCU_TRAFFIC_BYTES = {"row_growth": 33_260_800 + 8_704, "column": 14_577_152 + 0}
 
 
 def parse_args():
