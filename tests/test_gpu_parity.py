@@ -328,3 +328,39 @@ def test_direct_tma_off_for_unaligned_widths():
     m = lb.LeniaModule({"radius": 5}, 37, 23)  # row stride not a multiple of 16 bytes
     assert m.info()["direct_tma"] is False
     m.close()
+
+
+_CHAIN_SNIPPET = r"""
+import hashlib, sys
+sys.path.insert(0, {root!r})
+import life_simulation_b200 as lb
+from life_simulation_b200 import workloads as wl
+w, h = 384, 216
+p = wl.fft3_params(w, h)
+p["noiseAmount"] = 0.05
+m = lb.LeniaModule(p, w, h)
+m.reset(11)
+m.upload(wl.patches(w, h, 6, 40, seed=3))
+for f in range(4):
+    m.encode(f, 3)
+print(hashlib.sha256(m.field().tobytes()).hexdigest())
+"""
+
+
+def test_chained_launches_change_no_bits():
+    """Consecutive spectral passes launched with programmatic dependent
+    launch (the default) and in plain stream order (LENIA_CHAINED_LAUNCH=0,
+    read once per process, so each setting runs in its own process) give the
+    same field bit for bit."""
+    import subprocess
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    code = _CHAIN_SNIPPET.format(root=root)
+    out = {}
+    for env in ("1", "0"):
+        e = dict(os.environ, LENIA_CHAINED_LAUNCH=env)
+        r = subprocess.run([sys.executable, "-c", code], env=e, capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stderr[-2000:]
+        out[env] = r.stdout.strip().splitlines()[-1]
+    assert out["1"] == out["0"]
