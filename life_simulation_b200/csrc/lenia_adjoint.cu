@@ -151,6 +151,21 @@ __global__ void __launch_bounds__(RowK<PI, RB>::T, (512 / RowK<PI, RB>::T > 1 ? 
             ok[it] = q < RB * NRC && bi[it] < rows;
         }
         const auto gidx = [&](int it, int t) { return size_t(y0 + bi[it]) * W + 2 * (jj[it] + t * NRC); };
+        // The potentials of step t (kept by the recomputation's row pass) at
+        // this thread's pixel pairs, one kernel ahead: kernel 0's are in
+        // flight during the inverse row transform below, kernel k+1's during
+        // kernel k's forward transform.
+        float2 zn[ITL][RC];
+        const auto fetch_u = [&](int kk) {
+            const float* Uk = sw.U + size_t(kk) * H * W;
+#pragma unroll
+            for (int it = 0; it < ITL; ++it) {
+                if (!ok[it]) continue;
+#pragma unroll
+                for (int t = 0; t < RC; ++t) zn[it][t] = __ldg(reinterpret_cast<const float2*>(Uk + gidx(it, t)));
+            }
+        };
+        if (has_q && nk > 0) fetch_u(0);
         // dL/dA_{t+1} at this thread's pixel pairs (2n, 2n+1), n = j + t*NRC.
         float2 gv[ITL][RC];
         if (sw.SG) {
@@ -209,8 +224,6 @@ __global__ void __launch_bounds__(RowK<PI, RB>::T, (512 / RowK<PI, RB>::T > 1 ? 
         // The dt and mode-1 terms are linear in the kernels' contributions,
         // so they are summed kernel by kernel (no per-pixel accumulator).
         for (int kk = 0; kk < nk; ++kk) {
-            // The potentials of step t, kept by the recomputation's row pass.
-            const float* Uk = sw.U + size_t(kk) * H * W;
             const auto pick = [&](const float(&v)[kMaxKernels]) {
                 return kk == 0 ? v[0] : kk == 1 ? v[1] : kk == 2 ? v[2] : v[3];
             };
@@ -223,7 +236,7 @@ __global__ void __launch_bounds__(RowK<PI, RB>::T, (512 / RowK<PI, RB>::T > 1 ? 
                 if (!ok[it]) continue;
                 float2 z[RC];
 #pragma unroll
-                for (int t = 0; t < RC; ++t) z[t] = __ldg(reinterpret_cast<const float2*>(Uk + gidx(it, t)));
+                for (int t = 0; t < RC; ++t) z[t] = zn[it][t];
 #pragma unroll
                 for (int t = 0; t < RC; ++t) {
                     float qv[2];
@@ -251,6 +264,7 @@ __global__ void __launch_bounds__(RowK<PI, RB>::T, (512 / RowK<PI, RB>::T > 1 ? 
                     zq[it][t] = make_float2(qv[0], qv[1]);
                 }
             }
+            if (kk + 1 < nk) fetch_u(kk + 1);
             block_add(&red[kk * kPerKernel + 0], pmu);
             block_add(&red[kk * kPerKernel + 1], psig);
             block_add(&red[kk * kPerKernel + 2], ph);
