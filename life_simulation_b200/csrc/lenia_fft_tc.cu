@@ -63,9 +63,28 @@ __global__ void __launch_bounds__(256)
     const float kscale = float(H) * float(H);  // 16^(2 NP)
     const auto at = [](float2* buf) { return [buf](int b, int i, float2 v) { buf[b * PITCH + i] = v; }; };
     const auto from = [](const float2* buf) { return [buf](int b, int i) { return buf[b * PITCH + i]; }; };
+    // Product elements per thread; up to 16, their kernel spectrum values are
+    // fetched one kernel ahead into registers (kernel 0's during the forward
+    // transform, kernel k+1's during kernel k's inverse).
+    constexpr int PER = (B * H + T - 1) / T;
+    constexpr bool kAhead = PER <= 16;
     for (int k0 = blockIdx.x * B; k0 < M; k0 += gridDim.x * B) {
         const int cols = min(B, M - k0);
         const size_t gbase = size_t(k0 / KB) * H * KB + (k0 % KB);
+        float kv[kAhead ? PER : 1];
+        const auto fetch_k = [&](int kk) {
+            if constexpr (kAhead) {
+                const float* kh = khat + size_t(kk) * (M + 1) * Hh;
+#pragma unroll
+                for (int j = 0; j < PER; ++j) {
+                    const int idx = int(threadIdx.x) + j * T;
+                    const int b = idx % B, ky = idx / B;
+                    const int kyr = min(ky, H - ky);
+                    kv[j] = (idx < B * H && b < cols) ? __ldg(kh + size_t(k0 + b) * Hh + kyr) : 0.0f;
+                }
+            }
+        };
+        if (nk > 0) fetch_k(0);
         // Forward column FFT: global -> X (-> Y) -> Cb.
         tcfft::pass16<PF, 0, false, PREC, B, T>(
             [&](int b, int i) { return __ldg(S + gbase + size_t(i) * KB + b); }, at(X), twf, Ff, cols);
@@ -81,22 +100,35 @@ __global__ void __launch_bounds__(256)
         for (int kk = 0; kk < nk; ++kk) {
             const float* kh = khat + size_t(kk) * (M + 1) * Hh;
             // Spectrum product (packed column 0 split with C[k] and conj C[-k]).
-            for (int idx = threadIdx.x; idx < B * H; idx += T) {
+            const auto product = [&](int idx, float kval) {
                 const int b = idx % B, ky = idx / B;
-                if (b >= cols) continue;
                 const int kx = k0 + b;
                 const int kyr = min(ky, H - ky);
                 const float2 c = Cb[b * PITCH + ky];
                 float2 d;
                 if (kx == 0) {
-                    const float P = __ldg(kh + kyr), Q = __ldg(kh + size_t(M) * Hh + kyr);
+                    const float P = kval, Q = __ldg(kh + size_t(M) * Hh + kyr);
                     const float2 cm = cconj(Cb[ky == 0 ? 0 : H - ky]);
                     d = cadd(cscale(c, 0.5f * (P + Q)), cscale(cm, 0.5f * (P - Q)));
                 } else {
-                    d = cscale(c, __ldg(kh + size_t(kx) * Hh + kyr));
+                    d = cscale(c, kval);
                 }
                 X[b * PITCH + ky] = cscale(d, kscale);
+            };
+            if constexpr (kAhead) {
+#pragma unroll
+                for (int j = 0; j < PER; ++j) {
+                    const int idx = int(threadIdx.x) + j * T;
+                    if (idx < B * H && idx % B < cols) product(idx, kv[j]);
+                }
+            } else {
+                for (int idx = threadIdx.x; idx < B * H; idx += T) {
+                    const int b = idx % B, ky = idx / B;
+                    if (b >= cols) continue;
+                    product(idx, __ldg(kh + size_t(k0 + b) * Hh + min(ky, H - ky)));
+                }
             }
+            if (kk + 1 < nk) fetch_k(kk + 1);
             __syncthreads();
             // Inverse column FFT: X -> Y (-> X) -> U_k (global).
             float2* dst = U + size_t(kk) * M * H + gbase;
