@@ -86,8 +86,12 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, i
 constexpr uint32_t kTmaPolls = 1u << 22;
 
 // One output tile at (x0, y0) of one world. `tmap` (or null): the state's
-// halo-tile tensor map; `err` counts halo loads whose wait ran out.
-template <int TW, int TH, int NK>
+// halo-tile tensor map; `err` counts halo loads whose wait ran out. S > 1
+// splits the kernel rows over S thread groups (group s takes rows dy = s,
+// s + S, ...) for fields too small to fill the GPU one thread per 8 outputs:
+// the groups' partial sums meet in shared memory and are added in group
+// order before the epilogue.
+template <int TW, int TH, int NK, int S = 1>
 __device__ __forceinline__ void direct_tile(const float* __restrict__ src, float* __restrict__ dst,
                                             const float* __restrict__ weights,  // [NK][2R+1][WP], zero padded
                                             const uint32_t* __restrict__ spans, // [NK][2R+1]
@@ -103,7 +107,10 @@ __device__ __forceinline__ void direct_tile(const float* __restrict__ src, float
 
     const int W = int(p.width), H = int(p.height);
     const int tid = threadIdx.x;
-    constexpr int NT = DirectTile<TW, TH>::kThreads;
+    constexpr int NT0 = DirectTile<TW, TH>::kThreads;  // threads per row group
+    constexpr int NT = NT0 * S;
+    const int grp = S > 1 ? tid / NT0 : 0;
+    const int lt = tid - grp * NT0;
 
     // Stage the halo tile: tile[r][c] = A[(y0 - R + r) mod H][(x0 - XP + c) mod W].
     // A box inside the field is one TMA load (its TR x TP layout is the
@@ -150,7 +157,7 @@ __device__ __forceinline__ void direct_tile(const float* __restrict__ src, float
     }
     __syncthreads();
 
-    const int tx = tid % (TW / PX), ty = tid / (TW / PX);
+    const int tx = lt % (TW / PX), ty = lt / (TW / PX);
     const int ox = tx * PX;  // first output column within the tile
     float acc[NK][PX];
 #pragma unroll
@@ -160,7 +167,7 @@ __device__ __forceinline__ void direct_tile(const float* __restrict__ src, float
 
 #pragma unroll
     for (int k = 0; k < NK; ++k) {
-        for (int dyi = 0; dyi < g.ksize; ++dyi) {
+        for (int dyi = grp; dyi < g.ksize; dyi += S) {
             int start, count;
             unpack_span(sp[k * g.ksize + dyi], start, count);
             // Input row for kernel row dy = dyi - R of output row ty.
@@ -183,6 +190,22 @@ __device__ __forceinline__ void direct_tile(const float* __restrict__ src, float
         }
     }
 
+    if constexpr (S > 1) {
+        float* part = reinterpret_cast<float*>(sp + NK * g.ksize);  // [S-1][NK][NT0][PX]
+        if (grp > 0) {
+#pragma unroll
+            for (int k = 0; k < NK; ++k)
+#pragma unroll
+                for (int j = 0; j < PX; ++j) part[(((grp - 1) * NK + k) * NT0 + lt) * PX + j] = acc[k][j];
+        }
+        __syncthreads();
+        if (grp > 0) return;
+        for (int q = 1; q < S; ++q)
+#pragma unroll
+            for (int k = 0; k < NK; ++k)
+#pragma unroll
+                for (int j = 0; j < PX; ++j) acc[k][j] += part[(((q - 1) * NK + k) * NT0 + lt) * PX + j];
+    }
     const int gy = y0 + ty;
     if (gy >= H) return;
     const float* arow = tile + (ty + g.r) * TP + ox + g.xp;
@@ -199,14 +222,14 @@ __device__ __forceinline__ void direct_tile(const float* __restrict__ src, float
     }
 }
 
-template <int TW, int TH, int NK>
-__global__ void __launch_bounds__(DirectTile<TW, TH>::kThreads)
+template <int TW, int TH, int NK, int S>
+__global__ void __launch_bounds__(DirectTile<TW, TH>::kThreads * S)
     direct_step_kernel(const float* __restrict__ src, float* __restrict__ dst,
                        const float* __restrict__ weights, const uint32_t* __restrict__ spans,
                        DirectGeometry g, StepParams p, const __grid_constant__ CUtensorMap tmap, int use_tma,
                        int* err) {
-    direct_tile<TW, TH, NK>(src, dst, weights, spans, g, p, blockIdx.x * TW, blockIdx.y * TH,
-                            use_tma ? &tmap : nullptr, err);
+    direct_tile<TW, TH, NK, S>(src, dst, weights, spans, g, p, blockIdx.x * TW, blockIdx.y * TH,
+                               use_tma ? &tmap : nullptr, err);
 }
 
 // Many worlds in one launch: CTA i computes tile tiles[i] = (world, tile x,
@@ -222,14 +245,15 @@ __global__ void __launch_bounds__(DirectTile<TW, TH>::kThreads)
     direct_tile<TW, TH, 1>(w.src, w.dst, w.weights, w.spans, w.g, w.p, t.y * TW, t.z * TH, nullptr, nullptr);
 }
 
-template <int TW, int TH, int NK>
+template <int TW, int TH, int NK, int S>
 cudaError_t launch_t(const float* src, float* dst, const float* weights, const uint32_t* spans,
                      const DirectGeometry& g, const StepParams& p, cudaStream_t stream, const DirectTma* tma,
                      int buffer) {
     const int TP = TW + 2 * g.xp + 8;
     const size_t smem = sizeof(float) * (size_t(TH + 2 * g.r) * TP + size_t(NK) * g.ksize * g.wp) +
-                        sizeof(uint32_t) * NK * g.ksize;
-    auto fn = direct_step_kernel<TW, TH, NK>;
+                        sizeof(uint32_t) * NK * g.ksize +
+                        sizeof(float) * size_t(S - 1) * NK * DirectTile<TW, TH>::kThreads * PX;
+    auto fn = direct_step_kernel<TW, TH, NK, S>;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;
     CUtensorMap map;
@@ -237,20 +261,20 @@ cudaError_t launch_t(const float* src, float* dst, const float* weights, const u
     const bool on = tma && tma->on && (buffer == 0 || buffer == 1);
     if (on) std::memcpy(&map, tma->map[buffer], sizeof map);
     dim3 grid((p.width + TW - 1) / TW, (p.height + TH - 1) / TH);
-    fn<<<grid, DirectTile<TW, TH>::kThreads, smem, stream>>>(src, dst, weights, spans, g, p, map, on ? 1 : 0,
-                                                             on ? tma->err : nullptr);
+    fn<<<grid, DirectTile<TW, TH>::kThreads * S, smem, stream>>>(src, dst, weights, spans, g, p, map, on ? 1 : 0,
+                                                                 on ? tma->err : nullptr);
     return cudaGetLastError();
 }
 
-template <int TW, int TH>
+template <int TW, int TH, int S>
 cudaError_t launch_nk(int nk, const float* src, float* dst, const float* weights,
                       const uint32_t* spans, const DirectGeometry& g, const StepParams& p,
                       cudaStream_t s, const DirectTma* tma, int buffer) {
     switch (nk) {
-    case 1: return launch_t<TW, TH, 1>(src, dst, weights, spans, g, p, s, tma, buffer);
-    case 2: return launch_t<TW, TH, 2>(src, dst, weights, spans, g, p, s, tma, buffer);
-    case 3: return launch_t<TW, TH, 3>(src, dst, weights, spans, g, p, s, tma, buffer);
-    case 4: return launch_t<TW, TH, 4>(src, dst, weights, spans, g, p, s, tma, buffer);
+    case 1: return launch_t<TW, TH, 1, S>(src, dst, weights, spans, g, p, s, tma, buffer);
+    case 2: return launch_t<TW, TH, 2, S>(src, dst, weights, spans, g, p, s, tma, buffer);
+    case 3: return launch_t<TW, TH, 3, S>(src, dst, weights, spans, g, p, s, tma, buffer);
+    case 4: return launch_t<TW, TH, 4, S>(src, dst, weights, spans, g, p, s, tma, buffer);
     default: return cudaErrorInvalidValue;
     }
 }
@@ -275,13 +299,26 @@ size_t direct_smem_bytes(int tile_cfg, int nk, const DirectGeometry& g) {
 cudaError_t launch_direct_step(int tile_cfg, int nk, const float* src, float* dst,
                                const float* weights, const uint32_t* spans,
                                const DirectGeometry& g, const StepParams& p,
-                               cudaStream_t stream, const DirectTma* tma, int buffer) {
+                               cudaStream_t stream, const DirectTma* tma, int buffer, int split) {
+    if (tile_cfg == kDirectTile32x16) {
+        switch (split) {
+        case 1: return launch_nk<32, 16, 1>(nk, src, dst, weights, spans, g, p, stream, tma, buffer);
+        case 2: return launch_nk<32, 16, 2>(nk, src, dst, weights, spans, g, p, stream, tma, buffer);
+        case 4: return launch_nk<32, 16, 4>(nk, src, dst, weights, spans, g, p, stream, tma, buffer);
+        case 8: return launch_nk<32, 16, 8>(nk, src, dst, weights, spans, g, p, stream, tma, buffer);
+        default: return cudaErrorInvalidValue;
+        }
+    }
+    if (split != 1) return cudaErrorInvalidValue;
     switch (tile_cfg) {
-    case kDirectTile32x16: return launch_nk<32, 16>(nk, src, dst, weights, spans, g, p, stream, tma, buffer);
-    case kDirectTile64x16: return launch_nk<64, 16>(nk, src, dst, weights, spans, g, p, stream, tma, buffer);
-    case kDirectTile64x32: return launch_nk<64, 32>(nk, src, dst, weights, spans, g, p, stream, tma, buffer);
+    case kDirectTile64x16: return launch_nk<64, 16, 1>(nk, src, dst, weights, spans, g, p, stream, tma, buffer);
+    case kDirectTile64x32: return launch_nk<64, 32, 1>(nk, src, dst, weights, spans, g, p, stream, tma, buffer);
     default: return cudaErrorInvalidValue;
     }
+}
+
+size_t direct_split_smem_bytes(int split, int nk) {
+    return sizeof(float) * size_t(split - 1) * nk * DirectTile<32, 16>::kThreads * PX;
 }
 
 bool direct_tma_encode(int tile_cfg, const DirectGeometry& g, float* const fields[2], int w, int h, DirectTma& out) {

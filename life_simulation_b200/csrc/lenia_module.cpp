@@ -774,6 +774,19 @@ int LeniaModule::buildDirectTables() {
     else if (tiles(64, 16) >= 2 * sms) direct_tile_ = kDirectTile64x16;
     else direct_tile_ = kDirectTile32x16;
     if (direct_smem_bytes(direct_tile_, direct_nk_, dgeo_) > 220 * 1024) direct_tile_ = kDirectTile32x16;
+    // A field too small to give ~16 warps per SM at one thread per 8 outputs
+    // (64 threads per 32x16 tile) splits each tile's kernel rows over up to 8
+    // thread groups. A size rule, not a timing, so a configuration always
+    // sums in the same order (the same bits run to run).
+    direct_split_ = 1;
+    if (direct_tile_ == kDirectTile32x16) {
+        const int warps = tiles(32, 16) * 2;
+        while (direct_split_ < 8 && 2 * direct_split_ <= dgeo_.ksize && warps * direct_split_ < 16 * sms)
+            direct_split_ *= 2;
+        while (direct_split_ > 1 && direct_smem_bytes(direct_tile_, direct_nk_, dgeo_) +
+                                            direct_split_smem_bytes(direct_split_, direct_nk_) > 220 * 1024)
+            direct_split_ /= 2;
+    }
     // Halo tiles by TMA where the size allows it (interior tiles only).
     // LENIA_DIRECT_TMA in the environment at setup: 0 keeps element loads,
     // 1 uses TMA wherever the size allows; unset, the faster one here.
@@ -801,7 +814,7 @@ int LeniaModule::buildDirectTables() {
                 cudaEventRecord(a, stream_);
                 for (int i = 0; i < 3; ++i)
                     launch_direct_step(direct_tile_, direct_nk_, field_[0], field_[1], d_weights_, d_spans_, dgeo_, p,
-                                       stream_, v ? &direct_tma_ : nullptr, 0);
+                                       stream_, v ? &direct_tma_ : nullptr, 0, direct_split_);
                 cudaEventRecord(b, stream_);
                 cudaEventSynchronize(b);
                 float ms = 0.0f;
@@ -1235,7 +1248,7 @@ int LeniaModule::stepImpl(const lenia_frame_params& fp, uint32_t substeps, cudaS
         } else {
             e = launch(LENIA_PHASE_DIRECT, s, [&] {
                 return launch_direct_step(direct_tile_, direct_nk_, src, dst, d_weights_, d_spans_, dgeo_, p, s,
-                                          &direct_tma_, cur_);
+                                          &direct_tma_, cur_, direct_split_);
             });
             if (e != cudaSuccess) return cudaFail(e, "direct step");
         }
@@ -1255,6 +1268,7 @@ void LeniaModule::info(lenia_info* o) const {
     o->device_bytes = device_bytes_;
     o->fft_precision = tc_precision_;
     o->direct_tma = (!use_fft_ && direct_tma_.on) ? 1u : 0u;
+    o->direct_split = use_fft_ ? 0u : uint32_t(direct_split_);
     if (use_fft_) {
         for (int i = 0; i < fgeo_.row.npass && i < 8; ++i) o->fft_radix_row[i] = uint32_t(fgeo_.row.radix[i]);
         for (int i = 0; i < fgeo_.col.npass && i < 8; ++i) o->fft_radix_col[i] = uint32_t(fgeo_.col.radix[i]);

@@ -204,6 +204,7 @@ private:
     DirectGeometry dgeo_{};
     int direct_tile_ = kDirectTile64x16;
     int direct_nk_ = 1;
+    int direct_split_ = 1;  // kernel-row thread groups per tile (small fields)
     FftGeometry fgeo_{};
     bool fast_col_ = false, fast_row_ = false;  // compile-time-plan passes
     int col_batch_ = 2, row_batch_ = 2;         // autotuned per size

@@ -324,6 +324,17 @@ def test_direct_tma_halo_tiles_equal_element_loads(monkeypatch, w, h, radius):
     np.testing.assert_array_equal(out[0], out[1])
 
 
+def test_direct_split_for_small_fields():
+    """Small fields split each tile's kernel rows over several thread groups
+    (a size rule: the same configuration always sums in the same order)."""
+    small = lb.LeniaModule(wl.workload("single_256")[0], 256, 256)
+    assert small.info()["direct_split"] == 8
+    big = lb.LeniaModule({"radius": 13}, 1920, 1080)
+    assert big.info()["direct_split"] == 1
+    small.close()
+    big.close()
+
+
 def test_direct_tma_off_for_unaligned_widths():
     m = lb.LeniaModule({"radius": 5}, 37, 23)  # row stride not a multiple of 16 bytes
     assert m.info()["direct_tma"] is False
