@@ -35,9 +35,10 @@ pixels x steps; ``value`` is whole-job Mpixel-steps/s.
   (a radix-16 stage as a real 32x32 GEMM: 128 FLOP per point, x3 hi/lo).
 * library_fft_baseline: the same step from torch.fft (cuFFT) and torch ops
   in one CUDA graph, same flush protocol: a library comparator.
-* published_config: 1024x512, 3 kernels R=24 -- the one FFT configuration
-  the reference publishes a time for (Apple M5 Max, README.md:47-48) --
-  timed the same way, beside that published figure.
+* published_config / published_direct_config: 1024x512, 3 kernels R=24 (FFT)
+  and 1280x720, 1 kernel R=32 (direct) -- the two Lenia configurations the
+  reference publishes times for (Apple M5 Max, README.md:47-48) -- timed the
+  same way, beside those published figures.
 * --impl reference: that CPU reference alone, as the reference arm.
 """
 from __future__ import annotations
@@ -193,6 +194,46 @@ def cpu_baseline_port(params, w, h, init, seconds):
             break
     return {"value": w * h * steps / el / 1e6, "unit": UNIT, "cores": 1, "kind": "port",
             "sample": f"full {w}x{h} field, {steps} substeps in {el:.1f} s (FP64 oracle)"}
+
+
+def published_direct_bench(steps: int = 50, warmup: int = 5) -> dict:
+    """The reference's published direct configuration: one kernel, R=32,
+    1280x720 (README.md:47-48, 19.4 ms per frame on an Apple M5 Max, one
+    substep per frame); the module's default kernel shell, seeded patches.
+    Timed like the value region."""
+    import torch
+
+    import life_simulation_b200 as lb
+    from life_simulation_b200 import workloads as wl
+
+    w, h = 1280, 720
+    m = lb.LeniaModule({"radius": 32, "convMode": "direct"}, w, h)
+    m.reset(2)
+    m.upload(wl.patches(w, h, 12, 96, seed=2))
+    stream = torch.cuda.Stream()
+    sh = stream.cuda_stream
+    fp = m.frame_params(0)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    evs = []
+    with torch.cuda.stream(stream):
+        for i in range(warmup + steps):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            m.step(fp, 1, sh)
+            b.record(stream)
+            if i >= warmup:
+                evs.append((a, b))
+    torch.cuda.synchronize()
+    ms = float(np.mean([a.elapsed_time(b) for a, b in evs]))
+    info = m.info()
+    m.close()
+    ref_ms = 19.4
+    return {"workload": "direct, 1 kernel R=32, 1280x720 (the reference's published direct configuration)",
+            "ms_per_step": ms, "value": w * h / (ms / 1e3) / 1e6, "unit": UNIT,
+            "direct_tma": info["direct_tma"], "direct_split": info["direct_split"],
+            "reference_published": {"ms_per_frame": ref_ms, "value": w * h / (ref_ms / 1e3) / 1e6,
+                                    "hardware": "Apple M5 Max (Metal), README.md:47-48; not reproducible here"}}
 
 
 def published_config_bench(steps: int = 100, warmup: int = 5) -> dict:
@@ -546,6 +587,7 @@ def run_b200(args):
         line["library_fft_baseline"] = library_fft_baseline(params, w, h, init)
     if rank == 0 and world == 1 and args.workload == WORKLOAD:
         line["published_config"] = published_config_bench()
+        line["published_direct_config"] = published_direct_bench()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_baseline(params, w, h, init, args.cpu_seconds)
