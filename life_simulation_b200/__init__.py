@@ -81,7 +81,8 @@ class Info(ctypes.Structure):
                 ("num_kernels", ctypes.c_uint32), ("use_stamp_init", ctypes.c_uint32),
                 ("device_bytes", ctypes.c_uint64), ("fft_radix_row", ctypes.c_uint32 * 8),
                 ("fft_radix_col", ctypes.c_uint32 * 8), ("fft_precision", ctypes.c_uint32),
-                ("direct_tma", ctypes.c_uint32), ("direct_split", ctypes.c_uint32)]
+                ("direct_tma", ctypes.c_uint32), ("direct_split", ctypes.c_uint32),
+                ("direct_outputs_per_thread", ctypes.c_uint32)]
 
 
 # Every symbol include/lenia_b200.h declares (checked by the CPU tests).
@@ -492,7 +493,8 @@ class LeniaModule:
                 "device_bytes": i.device_bytes,
                 "fft_radix_row": [r for r in i.fft_radix_row if r],
                 "fft_radix_col": [r for r in i.fft_radix_col if r], "fft_precision": i.fft_precision,
-                "direct_tma": bool(i.direct_tma), "direct_split": i.direct_split}
+                "direct_tma": bool(i.direct_tma), "direct_split": i.direct_split,
+                "direct_outputs_per_thread": i.direct_outputs_per_thread}
 
 
 def inspect(params, scene_w: int, scene_h: int, base_dir: Optional[str] = None) -> dict:

@@ -33,11 +33,14 @@ namespace lenia {
 
 namespace {
 
-constexpr int PX = 8;  // outputs per thread along x
+constexpr int PX = 8;  // taps per chunk along x (and the default outputs per thread)
 
-template <int TW, int TH>
+// OX outputs per thread along x: 8, or 16 on large tiles (half the input
+// loads per multiply-add; each output's sum runs in the same order either
+// way, so the two give the same bits).
+template <int TW, int TH, int OX = PX>
 struct DirectTile {
-    static constexpr int kThreads = (TW / PX) * TH;
+    static constexpr int kThreads = (TW / OX) * TH;
 };
 
 // Per-kernel-row chunk plan, filled on the host: for row dy (0..2R), the first
@@ -91,7 +94,7 @@ constexpr uint32_t kTmaPolls = 1u << 22;
 // s + S, ...) for fields too small to fill the GPU one thread per 8 outputs:
 // the groups' partial sums meet in shared memory and are added in group
 // order before the epilogue.
-template <int TW, int TH, int NK, int S = 1>
+template <int TW, int TH, int NK, int S = 1, int OX = PX>
 __device__ __forceinline__ void direct_tile(const float* __restrict__ src, float* __restrict__ dst,
                                             const float* __restrict__ weights,  // [NK][2R+1][WP], zero padded
                                             const uint32_t* __restrict__ spans, // [NK][2R+1]
@@ -107,7 +110,7 @@ __device__ __forceinline__ void direct_tile(const float* __restrict__ src, float
 
     const int W = int(p.width), H = int(p.height);
     const int tid = threadIdx.x;
-    constexpr int NT0 = DirectTile<TW, TH>::kThreads;  // threads per row group
+    constexpr int NT0 = DirectTile<TW, TH, OX>::kThreads;  // threads per row group
     constexpr int NT = NT0 * S;
     const int grp = S > 1 ? tid / NT0 : 0;
     const int lt = tid - grp * NT0;
@@ -157,13 +160,13 @@ __device__ __forceinline__ void direct_tile(const float* __restrict__ src, float
     }
     __syncthreads();
 
-    const int tx = lt % (TW / PX), ty = lt / (TW / PX);
-    const int ox = tx * PX;  // first output column within the tile
-    float acc[NK][PX];
+    const int tx = lt % (TW / OX), ty = lt / (TW / OX);
+    const int ox = tx * OX;  // first output column within the tile
+    float acc[NK][OX];
 #pragma unroll
     for (int k = 0; k < NK; ++k)
 #pragma unroll
-        for (int j = 0; j < PX; ++j) acc[k][j] = 0.0f;
+        for (int j = 0; j < OX; ++j) acc[k][j] = 0.0f;
 
 #pragma unroll
     for (int k = 0; k < NK; ++k) {
@@ -177,26 +180,32 @@ __device__ __forceinline__ void direct_tile(const float* __restrict__ src, float
                 const int d0 = start + c * PX;  // multiple of 4
                 const float4* ip = reinterpret_cast<const float4*>(in_row + d0);
                 const float4* wp = reinterpret_cast<const float4*>(w_row + d0);
-                float4 a0 = ip[0], a1 = ip[1], a2 = ip[2], a3 = ip[3];
-                float4 w0 = wp[0], w1 = wp[1];
-                const float in[16] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w,
-                                      a2.x, a2.y, a2.z, a2.w, a3.x, a3.y, a3.z, a3.w};
+                float in[OX + PX];
+#pragma unroll
+                for (int q = 0; q < (OX + PX) / 4; ++q) {
+                    const float4 a = ip[q];
+                    in[4 * q] = a.x;
+                    in[4 * q + 1] = a.y;
+                    in[4 * q + 2] = a.z;
+                    in[4 * q + 3] = a.w;
+                }
+                const float4 w0 = wp[0], w1 = wp[1];
                 const float wv[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
 #pragma unroll
                 for (int i = 0; i < PX; ++i)
 #pragma unroll
-                    for (int j = 0; j < PX; ++j) acc[k][j] = fmaf(wv[i], in[i + j], acc[k][j]);
+                    for (int j = 0; j < OX; ++j) acc[k][j] = fmaf(wv[i], in[i + j], acc[k][j]);
             }
         }
     }
 
     if constexpr (S > 1) {
-        float* part = reinterpret_cast<float*>(sp + NK * g.ksize);  // [S-1][NK][NT0][PX]
+        float* part = reinterpret_cast<float*>(sp + NK * g.ksize);  // [S-1][NK][NT0][OX]
         if (grp > 0) {
 #pragma unroll
             for (int k = 0; k < NK; ++k)
 #pragma unroll
-                for (int j = 0; j < PX; ++j) part[(((grp - 1) * NK + k) * NT0 + lt) * PX + j] = acc[k][j];
+                for (int j = 0; j < OX; ++j) part[(((grp - 1) * NK + k) * NT0 + lt) * OX + j] = acc[k][j];
         }
         __syncthreads();
         if (grp > 0) return;
@@ -204,13 +213,13 @@ __device__ __forceinline__ void direct_tile(const float* __restrict__ src, float
 #pragma unroll
             for (int k = 0; k < NK; ++k)
 #pragma unroll
-                for (int j = 0; j < PX; ++j) acc[k][j] += part[(((q - 1) * NK + k) * NT0 + lt) * PX + j];
+                for (int j = 0; j < OX; ++j) acc[k][j] += part[(((q - 1) * NK + k) * NT0 + lt) * OX + j];
     }
     const int gy = y0 + ty;
     if (gy >= H) return;
     const float* arow = tile + (ty + g.r) * TP + ox + g.xp;
 #pragma unroll
-    for (int j = 0; j < PX; ++j) {
+    for (int j = 0; j < OX; ++j) {
         const int gx = x0 + ox + j;
         if (gx >= W) break;
         const float A = arow[j];
@@ -222,14 +231,14 @@ __device__ __forceinline__ void direct_tile(const float* __restrict__ src, float
     }
 }
 
-template <int TW, int TH, int NK, int S>
-__global__ void __launch_bounds__(DirectTile<TW, TH>::kThreads * S)
+template <int TW, int TH, int NK, int S, int OX>
+__global__ void __launch_bounds__(DirectTile<TW, TH, OX>::kThreads * S)
     direct_step_kernel(const float* __restrict__ src, float* __restrict__ dst,
                        const float* __restrict__ weights, const uint32_t* __restrict__ spans,
                        DirectGeometry g, StepParams p, const __grid_constant__ CUtensorMap tmap, int use_tma,
                        int* err) {
-    direct_tile<TW, TH, NK, S>(src, dst, weights, spans, g, p, blockIdx.x * TW, blockIdx.y * TH,
-                               use_tma ? &tmap : nullptr, err);
+    direct_tile<TW, TH, NK, S, OX>(src, dst, weights, spans, g, p, blockIdx.x * TW, blockIdx.y * TH,
+                                   use_tma ? &tmap : nullptr, err);
 }
 
 // Many worlds in one launch: CTA i computes tile tiles[i] = (world, tile x,
@@ -245,15 +254,15 @@ __global__ void __launch_bounds__(DirectTile<TW, TH>::kThreads)
     direct_tile<TW, TH, 1>(w.src, w.dst, w.weights, w.spans, w.g, w.p, t.y * TW, t.z * TH, nullptr, nullptr);
 }
 
-template <int TW, int TH, int NK, int S>
+template <int TW, int TH, int NK, int S, int OX>
 cudaError_t launch_t(const float* src, float* dst, const float* weights, const uint32_t* spans,
                      const DirectGeometry& g, const StepParams& p, cudaStream_t stream, const DirectTma* tma,
                      int buffer) {
     const int TP = TW + 2 * g.xp + 8;
     const size_t smem = sizeof(float) * (size_t(TH + 2 * g.r) * TP + size_t(NK) * g.ksize * g.wp) +
                         sizeof(uint32_t) * NK * g.ksize +
-                        sizeof(float) * size_t(S - 1) * NK * DirectTile<TW, TH>::kThreads * PX;
-    auto fn = direct_step_kernel<TW, TH, NK, S>;
+                        sizeof(float) * size_t(S - 1) * NK * DirectTile<TW, TH, OX>::kThreads * OX;
+    auto fn = direct_step_kernel<TW, TH, NK, S, OX>;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;
     CUtensorMap map;
@@ -261,20 +270,20 @@ cudaError_t launch_t(const float* src, float* dst, const float* weights, const u
     const bool on = tma && tma->on && (buffer == 0 || buffer == 1);
     if (on) std::memcpy(&map, tma->map[buffer], sizeof map);
     dim3 grid((p.width + TW - 1) / TW, (p.height + TH - 1) / TH);
-    fn<<<grid, DirectTile<TW, TH>::kThreads * S, smem, stream>>>(src, dst, weights, spans, g, p, map, on ? 1 : 0,
+    fn<<<grid, DirectTile<TW, TH, OX>::kThreads * S, smem, stream>>>(src, dst, weights, spans, g, p, map, on ? 1 : 0,
                                                                  on ? tma->err : nullptr);
     return cudaGetLastError();
 }
 
-template <int TW, int TH, int S>
+template <int TW, int TH, int S, int OX = PX>
 cudaError_t launch_nk(int nk, const float* src, float* dst, const float* weights,
                       const uint32_t* spans, const DirectGeometry& g, const StepParams& p,
                       cudaStream_t s, const DirectTma* tma, int buffer) {
     switch (nk) {
-    case 1: return launch_t<TW, TH, 1, S>(src, dst, weights, spans, g, p, s, tma, buffer);
-    case 2: return launch_t<TW, TH, 2, S>(src, dst, weights, spans, g, p, s, tma, buffer);
-    case 3: return launch_t<TW, TH, 3, S>(src, dst, weights, spans, g, p, s, tma, buffer);
-    case 4: return launch_t<TW, TH, 4, S>(src, dst, weights, spans, g, p, s, tma, buffer);
+    case 1: return launch_t<TW, TH, 1, S, OX>(src, dst, weights, spans, g, p, s, tma, buffer);
+    case 2: return launch_t<TW, TH, 2, S, OX>(src, dst, weights, spans, g, p, s, tma, buffer);
+    case 3: return launch_t<TW, TH, 3, S, OX>(src, dst, weights, spans, g, p, s, tma, buffer);
+    case 4: return launch_t<TW, TH, 4, S, OX>(src, dst, weights, spans, g, p, s, tma, buffer);
     default: return cudaErrorInvalidValue;
     }
 }
@@ -299,7 +308,12 @@ size_t direct_smem_bytes(int tile_cfg, int nk, const DirectGeometry& g) {
 cudaError_t launch_direct_step(int tile_cfg, int nk, const float* src, float* dst,
                                const float* weights, const uint32_t* spans,
                                const DirectGeometry& g, const StepParams& p,
-                               cudaStream_t stream, const DirectTma* tma, int buffer, int split) {
+                               cudaStream_t stream, const DirectTma* tma, int buffer, int split, int ox) {
+    if (ox == 16) {
+        if (tile_cfg != kDirectTile64x32 || split != 1) return cudaErrorInvalidValue;
+        return launch_nk<64, 32, 1, 16>(nk, src, dst, weights, spans, g, p, stream, tma, buffer);
+    }
+    if (ox != PX) return cudaErrorInvalidValue;
     if (tile_cfg == kDirectTile32x16) {
         switch (split) {
         case 1: return launch_nk<32, 16, 1>(nk, src, dst, weights, spans, g, p, stream, tma, buffer);

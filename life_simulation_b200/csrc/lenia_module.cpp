@@ -787,6 +787,37 @@ int LeniaModule::buildDirectTables() {
                                             direct_split_smem_bytes(direct_split_, direct_nk_) > 220 * 1024)
             direct_split_ /= 2;
     }
+    // Outputs per thread on 64x32 tiles: 8 or 16, whichever runs faster here
+    // (a few steps each on the context's own buffers; the same bits either way).
+    direct_ox_ = 8;
+    const char* ox_env = std::getenv("LENIA_DIRECT_OX");  // "8" / "16" at setup: force either
+    const int ox_forced = ox_env ? std::atoi(ox_env) : 0;
+    if (direct_tile_ == kDirectTile64x32 && ox_forced == 16) {
+        direct_ox_ = 16;
+    } else if (direct_tile_ == kDirectTile64x32 && ox_forced != 8) {
+        StepParams p{};
+        p.width = w_;
+        p.height = h_;
+        p.num_kernels = uint32_t(direct_nk_);
+        for (int k = 0; k < 4; ++k) p.sigma[k] = 1.0f;
+        cudaEvent_t a = takeEvent(), b = takeEvent();
+        float best[2] = {1e30f, 1e30f};
+        for (int rep = 0; rep < 3; ++rep)
+            for (int v = 0; v < 2; ++v) {
+                cudaEventRecord(a, stream_);
+                for (int i = 0; i < 3; ++i)
+                    launch_direct_step(direct_tile_, direct_nk_, field_[0], field_[1], d_weights_, d_spans_, dgeo_, p,
+                                       stream_, nullptr, 0, 1, v ? 16 : 8);
+                cudaEventRecord(b, stream_);
+                cudaEventSynchronize(b);
+                float ms = 0.0f;
+                if (cudaEventElapsedTime(&ms, a, b) == cudaSuccess && rep > 0) best[v] = std::min(best[v], ms);
+            }
+        event_pool_.push_back(a);
+        event_pool_.push_back(b);
+        if ((e = cudaGetLastError()) != cudaSuccess) return cudaFail(e, "direct shape choice");
+        if (best[1] < best[0]) direct_ox_ = 16;
+    }
     // Halo tiles by TMA where the size allows it (interior tiles only).
     // LENIA_DIRECT_TMA in the environment at setup: 0 keeps element loads,
     // 1 uses TMA wherever the size allows; unset, the faster one here.
@@ -814,7 +845,7 @@ int LeniaModule::buildDirectTables() {
                 cudaEventRecord(a, stream_);
                 for (int i = 0; i < 3; ++i)
                     launch_direct_step(direct_tile_, direct_nk_, field_[0], field_[1], d_weights_, d_spans_, dgeo_, p,
-                                       stream_, v ? &direct_tma_ : nullptr, 0, direct_split_);
+                                       stream_, v ? &direct_tma_ : nullptr, 0, direct_split_, direct_ox_);
                 cudaEventRecord(b, stream_);
                 cudaEventSynchronize(b);
                 float ms = 0.0f;
@@ -1248,7 +1279,7 @@ int LeniaModule::stepImpl(const lenia_frame_params& fp, uint32_t substeps, cudaS
         } else {
             e = launch(LENIA_PHASE_DIRECT, s, [&] {
                 return launch_direct_step(direct_tile_, direct_nk_, src, dst, d_weights_, d_spans_, dgeo_, p, s,
-                                          &direct_tma_, cur_, direct_split_);
+                                          &direct_tma_, cur_, direct_split_, direct_ox_);
             });
             if (e != cudaSuccess) return cudaFail(e, "direct step");
         }
@@ -1269,6 +1300,7 @@ void LeniaModule::info(lenia_info* o) const {
     o->fft_precision = tc_precision_;
     o->direct_tma = (!use_fft_ && direct_tma_.on) ? 1u : 0u;
     o->direct_split = use_fft_ ? 0u : uint32_t(direct_split_);
+    o->direct_outputs_per_thread = use_fft_ ? 0u : uint32_t(direct_ox_);
     if (use_fft_) {
         for (int i = 0; i < fgeo_.row.npass && i < 8; ++i) o->fft_radix_row[i] = uint32_t(fgeo_.row.radix[i]);
         for (int i = 0; i < fgeo_.col.npass && i < 8; ++i) o->fft_radix_col[i] = uint32_t(fgeo_.col.radix[i]);

@@ -185,7 +185,7 @@ def test_fft_extras_vs_ref32():
         assert np.abs(g - o).max() < 2e-5
 
 
-@pytest.mark.parametrize("w,h", [(256, 256), (120, 90), (384, 216)])
+@pytest.mark.parametrize("w,h", [(256, 256), (120, 90), (384, 216), (1920, 1080)])
 def test_direct_and_fft_agree_per_step(w, h):
     pf = wl.fft3_params(w, h)
     pd = wl.fft3_params(w, h, conv="directMulti")
@@ -333,6 +333,28 @@ def test_direct_split_for_small_fields():
     assert big.info()["direct_split"] == 1
     small.close()
     big.close()
+
+
+def test_direct_outputs_per_thread_give_the_same_bits(monkeypatch):
+    """Large direct fields (64x32 tiles) may run 16 outputs per thread instead
+    of 8; every output's sum runs in the same order, so the field is the same
+    bit for bit."""
+    w, h = 1920, 1080
+    p = wl.fft3_params(w, h, conv="directMulti")
+    p["noiseAmount"] = 0.05
+    init = wl.patches(w, h, 12, 96, seed=8)
+    out = []
+    for ox in ("8", "16"):
+        monkeypatch.setenv("LENIA_DIRECT_OX", ox)
+        m = lb.LeniaModule(p, w, h)
+        assert m.info()["direct_outputs_per_thread"] == int(ox)
+        m.reset(3)
+        m.upload(init)
+        for f in range(2):
+            m.encode(f, 2)
+        out.append(m.field())
+        m.close()
+    np.testing.assert_array_equal(out[0], out[1])
 
 
 def test_direct_tma_off_for_unaligned_widths():
