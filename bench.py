@@ -557,6 +557,12 @@ def run_b200(args):
     launch_ms = phases[dom]["ms"] / phases[dom]["count"]
     peak, peak_kind = measured_peaks()
     achieved = bytes_px[dom] * w * h / (launch_ms / 1e3) / 1e9
+    direct_flops = None
+    if dom == "direct":
+        # The direct convolution is FP32-FMA bound: 2 FLOP per nonzero tap
+        # plus ~12 for the growth map, per pixel and kernel.
+        info = m.info()
+        direct_flops = (2 * info["direct_taps"] + 12 * info["num_kernels"]) * w * h
     step_bytes = (20 + 10 * K) * w * h  # canonical three-sweep bytes per pixel-step
     mean_step_ms = total_ms / args.steps
     line = base_line(args, world, args.steps, args.warmup, w, h, params)
@@ -564,18 +570,27 @@ def run_b200(args):
         line["config"]["launch_shape"] = {"cols_per_cta": shape[0], "rows_per_cta": shape[1] & 0xFF,
                                           "rows_pipelined": bool(shape[1] & lb.ROWS_PIPELINED),
                                           "chosen_by": chosen_by}
+    if direct_flops is not None:
+        fp32_peak = 148 * 128 * 2 * 1.965e9 / 1e12  # nominal FP32 FMA TFLOP/s (no measured figure)
+        tflops = direct_flops / (launch_ms / 1e3) / 1e12
+        roofline = {"bound": "fp32", "kernel": dom, "achieved": tflops, "peak": fp32_peak,
+                    "peak_source": "nominal (148 SMs x 128 FP32 lanes x 2 x 1.965 GHz)", "unit": "TFLOP/s",
+                    "frac": tflops / fp32_peak, "traffic": None, "algorithmic_flops_per_launch": direct_flops,
+                    "launch_ms": launch_ms}
+    else:
+        roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                    "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                    "traffic": NCU_TRAFFIC_BYTES.get(dom),
+                    "algorithmic_bytes_per_launch": bytes_px[dom] * w * h,
+                    "launch_ms": launch_ms,
+                    "step": {"bytes": step_bytes, "achieved": step_bytes / (mean_step_ms / 1e3) / 1e9,
+                             "frac": step_bytes / (mean_step_ms / 1e3) / 1e9 / peak}}
     line.update({
         "value": value, "ms_per_step": mean_step_ms,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(w * h * 4),
                 "d2h_bytes_per_step": int(w * h * 4), "steps": e2e_steps},
         "gpu_launches": int(launches),
-        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
-                     "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": NCU_TRAFFIC_BYTES.get(dom),
-                     "algorithmic_bytes_per_launch": bytes_px[dom] * w * h,
-                     "launch_ms": launch_ms,
-                     "step": {"bytes": step_bytes, "achieved": step_bytes / (mean_step_ms / 1e3) / 1e9,
-                              "frac": step_bytes / (mean_step_ms / 1e3) / 1e9 / peak}},
+        "roofline": roofline,
         "phases_ms_per_step": {k: v["ms"] / prof_steps for k, v in phases.items()},
         "kernel_timing": f"per-launch CUDA events over {prof_steps} further flushed steps",
         "frame_with_colour_layer": render_line,

@@ -130,6 +130,7 @@ typedef struct lenia_info {
     uint32_t direct_tma;      /* 1: the direct path loads interior halo tiles by TMA */
     uint32_t direct_split;    /* direct path: thread groups sharing a tile's kernel rows (1, 2, 4, 8) */
     uint32_t direct_outputs_per_thread; /* direct path: 8, or 16 on large tiles where faster */
+    uint32_t direct_taps;     /* direct path: nonzero kernel taps summed over its kernels */
 } lenia_info;
 
 typedef struct lenia_ctx lenia_ctx;

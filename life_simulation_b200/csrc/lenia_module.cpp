@@ -733,6 +733,9 @@ int LeniaModule::buildDirectTables() {
     }
     direct_nk_ = int(luts.size());
     num_k_ = uint32_t(direct_nk_);
+    direct_taps_ = 0;
+    for (const auto& lut : luts)
+        for (float v : lut) direct_taps_ += v != 0.0f ? 1u : 0u;
     dgeo_.r = r;
     dgeo_.ksize = 2 * r + 1;
     dgeo_.xp = (r + 3) / 4 * 4;
@@ -1301,6 +1304,7 @@ void LeniaModule::info(lenia_info* o) const {
     o->direct_tma = (!use_fft_ && direct_tma_.on) ? 1u : 0u;
     o->direct_split = use_fft_ ? 0u : uint32_t(direct_split_);
     o->direct_outputs_per_thread = use_fft_ ? 0u : uint32_t(direct_ox_);
+    o->direct_taps = use_fft_ ? 0u : direct_taps_;
     if (use_fft_) {
         for (int i = 0; i < fgeo_.row.npass && i < 8; ++i) o->fft_radix_row[i] = uint32_t(fgeo_.row.radix[i]);
         for (int i = 0; i < fgeo_.col.npass && i < 8; ++i) o->fft_radix_col[i] = uint32_t(fgeo_.col.radix[i]);

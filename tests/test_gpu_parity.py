@@ -329,6 +329,7 @@ def test_direct_split_for_small_fields():
     (a size rule: the same configuration always sums in the same order)."""
     small = lb.LeniaModule(wl.workload("single_256")[0], 256, 256)
     assert small.info()["direct_split"] == 8
+    assert small.info()["direct_taps"] == 516  # exp core, R=13: 0 < d^2 < 169
     big = lb.LeniaModule({"radius": 13}, 1920, 1080)
     assert big.info()["direct_split"] == 1
     small.close()
