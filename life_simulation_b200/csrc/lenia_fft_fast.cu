@@ -278,6 +278,11 @@ __global__ void __launch_bounds__(RowK<PI, RB>::T, (512 / RowK<PI, RB>::T > 1 ? 
     const StepParams& p = sw.p;
     const bool asym = p.growth_mode == 1u;
     const bool jitter = p.mu_jitter > 0.0f;
+    // The Euler step's parameters in registers (the rare noise / injection
+    // path reads them from the shared block out of line).
+    const bool extras = p.noise_amount > 0.0f || p.inject_amount > 0.0f;
+    const float dt = p.dt, sum_w = p.sum_weights;
+    const bool sw_ok = sum_w > 1e-6f;
     // Item idx of a row group: the rows of U_idx for idx < nk, else of A.
     const auto stage = [&](float2* dst, int y, int idx) {
         if (y >= H) return;
@@ -386,10 +391,14 @@ __global__ void __launch_bounds__(RowK<PI, RB>::T, (512 / RowK<PI, RB>::T > 1 ? 
                     za[it][t] = a;
                     continue;
                 }
-                const float2 r =
-                    make_float2(growth_finish_lean(p, a.x, acc[it][t][0], acc[it][t][0], uint32_t(2 * n), uint32_t(gy)),
-                                growth_finish_lean(p, a.y, acc[it][t][1], acc[it][t][1], uint32_t(2 * n + 1),
-                                                   uint32_t(gy)));
+                // growth_finish_lean with the parameters in registers.
+                const auto finish = [&](float A, float s, uint32_t gx) {
+                    if (extras) return growth_finish_call(p, A, s, s, gx, uint32_t(gy));
+                    const float A2 = asym ? A + dt * ((sw_ok ? s / sum_w : A) - A) : A + dt * s;
+                    return fminf(fmaxf(A2, 0.0f), 1.0f);
+                };
+                const float2 r = make_float2(finish(a.x, acc[it][t][0], uint32_t(2 * n)),
+                                             finish(a.y, acc[it][t][1], uint32_t(2 * n + 1)));
                 *reinterpret_cast<float2*>(A_out + size_t(gy) * W + 2 * n) = r;
                 if constexpr (CM) palette_pair(sw.cm, r, sw.rgba + size_t(gy) * W + 2 * n);
                 za[it][t] = r;
