@@ -274,6 +274,7 @@ __global__ void __launch_bounds__(RowK<PI, RB>::T, (512 / RowK<PI, RB>::T > 1 ? 
     const float* __restrict__ A = sw.A;
     float* __restrict__ A_out = sw.A_out;
     float2* __restrict__ S_next = sw.S_next;
+    float* __restrict__ U_px = sw.U_px;
     const int H = int(sw.p.height), nk = sw.nk;
     const StepParams& p = sw.p;
     const bool asym = p.growth_mode == 1u;
@@ -343,8 +344,8 @@ __global__ void __launch_bounds__(RowK<PI, RB>::T, (512 / RowK<PI, RB>::T > 1 ? 
                 IL::template twiddle<true>(z, jj[it], twi);
                 Dft<RC, true>::run(z);
                 const uint32_t gy = uint32_t(y0 + bi[it]);
-                if (sw.U_px) {  // keep the potentials (the adjoint's recomputation)
-                    float* up = sw.U_px + (size_t(kk) * H + gy) * W;
+                if (U_px) {  // keep the potentials (the adjoint's recomputation)
+                    float* up = U_px + (size_t(kk) * H + gy) * W;
 #pragma unroll
                     for (int t = 0; t < RC; ++t) *reinterpret_cast<float2*>(up + 2 * (jj[it] + t * NRC)) = z[t];
                 }
