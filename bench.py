@@ -25,6 +25,8 @@ pixels x steps; ``value`` is whole-job Mpixel-steps/s.
   MEASURED_PEAKS.json.
 * cpu_baseline: the reference's own Lenia module and kernels compiled for
   the CPU (oracle/_ref), on a bounded row band of the same workload.
+* accuracy_vs_fp64 (with the CPU leg): max and RMS |A_gpu - A_fp64| of 5
+  steps of the workload, each from the GPU's field, against the FP64 oracle.
 * adjoint: the gradient form on 32 worlds of 512x512 (K=2, R=16, growth
   mode 1, T=64, checkpoints every 8): device time of the forward rollout and of the
   backward (recomputation included), CUDA events on the launching stream
@@ -347,6 +349,40 @@ def cpu_baseline(params, w, h, init, seconds):
     return cpu_baseline_port(params, w, h, init, seconds)
 
 
+def accuracy_vs_fp64(params, w, h, init, steps: int = 5) -> dict:
+    """Max and RMS |A_gpu - A_fp64| per step of the workload: every step,
+    the GPU module (through the C ABI) and the FP64 oracle both start from
+    the GPU's current field, so each figure is one step's error, not an
+    accumulated drift. Part of the CPU leg: the oracle only checks."""
+    import life_simulation_b200 as lb
+    from oracle import lenia_oracle as lo
+
+    m = lb.LeniaModule(params, w, h)
+    o = lo.OracleLenia(params, w, h, "f64")
+    m.reset(3)
+    o.reset(3)
+    m.upload(init)
+    o.set_initial_field(init)
+    o.encode(0)  # builds the oracle's kernels; its state is replaced below
+    fp = m.frame_params(0)
+    a = np.asarray(init, np.float32)
+    mx, rms = [], []
+    for s in range(steps):
+        fp.frame_index = fp.audio_frame = s
+        m.upload(a)
+        m.step(fp, 1)
+        g = m.field()
+        o.state = a.astype(np.float64)
+        o.step_once(o.frame_params(), lo.pcg_hash(o.seed_ ^ (s * 197)), s, s)
+        d = g.astype(np.float64) - o.state
+        mx.append(float(np.abs(d).max()))
+        rms.append(float(np.sqrt(np.mean(d * d))))
+        a = g
+    m.close()
+    return {"steps": steps, "max_abs": mx, "rms": rms, "bound": 1e-5,
+            "what": "per step from the GPU's field, FP32 GPU vs the FP64 oracle"}
+
+
 def base_line(args, n, steps, warmup, w, h, params):
     return {
         "metric": METRIC, "unit": UNIT, "n_gpus": n, "steps": steps, "warmup": warmup,
@@ -608,6 +644,10 @@ def run_b200(args):
             line["cpu_baseline"] = cpu_baseline(params, w, h, init, args.cpu_seconds)
         except Exception as e:  # the oracle is optional here; the GPU number stands
             line["cpu_baseline"] = {"value": None, "error": str(e)}
+        try:
+            line["accuracy_vs_fp64"] = accuracy_vs_fp64(params, w, h, init)
+        except Exception as e:
+            line["accuracy_vs_fp64"] = {"error": str(e)}
     if rank == 0:
         print(json.dumps(line))
     m.close()
