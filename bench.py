@@ -799,6 +799,7 @@ def run_sweep(args):
     import life_simulation_b200 as lb
     from life_simulation_b200 import workloads as wl
     from life_simulation_b200.shard import loads, partition, world_cost
+    from life_simulation_b200.sweep import is_alive
 
     rank, world, local = dist_env()
     if world > 1:
@@ -836,10 +837,16 @@ def run_sweep(args):
     cm = lb.colormap_from_params({})
     barrier()
     t0 = time.perf_counter()
+    acts = []
     for _ in range(4):
         b.step(60)
-        b.activity(cm)  # synchronising readback: the lab's luma activity per world
+        acts.append(b.activity(cm))  # synchronising readback: the lab's luma activity per world
     batched_s = time.perf_counter() - t0
+    # Per readback: the worlds' mean luma and luma variance, averaged over
+    # this rank's worlds, and how many pass the lab's alive rule.
+    activity = [{"step": 60 * (j + 1), "mean_luma": float(mean.mean()), "mean_var_luma": float((std * std).mean()),
+                 "alive": sum(1 for x, y in zip(mean, std) if is_alive(float(x), float(y)))}
+                for j, (mean, std) in enumerate(acts)]
     paths = [b.path(i) for i in range(len(worlds))]
     b.close()
     if world > 1:
@@ -893,6 +900,7 @@ def run_sweep(args):
         "unit": UNIT, "value": batched, "plain": plain, "speedup": batched / plain,
         "worlds": len(worlds), "pixels_per_step": px, "steps": 240,
         "direct_worlds": paths.count(lb.CONV_DIRECT), "fft_worlds": paths.count(lb.CONV_FFT),
+        "activity": activity,
         "timing": "wall clock incl. 4 activity readbacks (batched); plain: "
                   f"{plain_steps} substeps per world, worlds in sequence"}))
     return 0
