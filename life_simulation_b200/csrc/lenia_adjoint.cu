@@ -1102,6 +1102,7 @@ int lenia_adjoint_create(const lenia_adjoint_config* cfg, lenia_adjoint** out) {
 }
 
 int lenia_adjoint_destroy(lenia_adjoint* a) {
+    if (!a) return LENIA_ERR_INVALID_ARG;
     delete a;
     return LENIA_OK;
 }

@@ -2,6 +2,7 @@
 include/lenia_b200.h declares, and its host logic (parameter parsing and
 the reference's setup fallbacks) resolves like the reference. No compute
 call needs a device here."""
+import ctypes
 import json
 import os
 import re
@@ -117,3 +118,42 @@ def test_inspect_reference_presets():
 def test_inspect_bad_json():
     with pytest.raises(lb.LeniaError):
         lb.inspect("{not json", 64, 64)
+
+
+_CTYPES = {"uint32_t": ctypes.c_uint32, "int32_t": ctypes.c_int32, "int": ctypes.c_int, "size_t": ctypes.c_size_t,
+           "float": ctypes.c_float, "double": ctypes.c_double, "uint64_t": ctypes.c_uint64}
+
+
+def declared_signatures():
+    """(return type, name, [parameter types]) of every declaration."""
+    text = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
+    out = []
+    for ret, name, args in re.findall(r"^\s*((?:const\s+)?\w+\s*\**)\s*(lenia_\w+)\s*\(([^;]*?)\)\s*;", text,
+                                      flags=re.S | re.M):
+        params = [] if args.strip() in ("", "void") else [" ".join(a.split()) for a in args.split(",")]
+        types = [p.rsplit(" ", 1)[0] if "*" not in p else "ptr" for p in params]
+        out.append((" ".join(ret.split()), name, types))
+    return out
+
+
+def test_every_entry_point_rejects_null_arguments():
+    # Null handles and null pointers (zero sizes) come back as
+    # LENIA_ERR_INVALID_ARG before any device work; the message getters
+    # return a string for a null handle. A separate handle on the library
+    # keeps these argtypes apart from the package's.
+    L = ctypes.CDLL(lb.LIB_PATH)
+    sigs = declared_signatures()
+    assert {n for _, n, _ in sigs} == set(declared_functions())
+    checked = 0
+    for ret, name, types in sigs:
+        fn = getattr(L, name)
+        fn.argtypes = [ctypes.c_void_p if t == "ptr" else _CTYPES[t.replace("const ", "")] for t in types]
+        args = [None if t == "ptr" else 0 for t in types]
+        if ret == "int":
+            fn.restype = ctypes.c_int
+            assert fn(*args) == -1, name  # LENIA_ERR_INVALID_ARG
+            checked += 1
+        elif ret == "const char*" and name != "lenia_status_string":
+            fn.restype = ctypes.c_char_p
+            assert isinstance(fn(*args), bytes), name
+    assert checked >= 60
