@@ -638,6 +638,18 @@ int LeniaModule::resolve(uint32_t scene_w, uint32_t scene_h) {
     fgeo_.row = prow;
     fgeo_.col = pcol;
     num_k_ = multi ? uint32_t(std::max<size_t>(1, std::min<size_t>(4, kernels_.size()))) : 1u;
+    // The direct path's radius limit (buildDirectTables), here as well so
+    // that the host-only inspection reports what setup would.
+    if (!use_fft_ && !direct_multi_ && radius_ > uint32_t(kMaxRadius))
+        return fail(LENIA_ERR_UNSUPPORTED,
+                    "direct convolution supports radius <= 32 (got " + std::to_string(radius_) + ")");
+    if (!use_fft_ && direct_multi_) {
+        for (size_t k = 0; k < std::max<size_t>(1, std::min<size_t>(4, kernels_.size())); ++k) {
+            const float scale = kernels_.empty() ? 1.0f : kernels_[k].radius_scale;
+            if (!(float(radius_) * scale <= float(kMaxRadius)))
+                return fail(LENIA_ERR_UNSUPPORTED, "direct convolution supports kernel radius <= 32");
+        }
+    }
     if (!warn.empty()) {
         std::string m;
         for (const auto& w : warn) m += (m.empty() ? "" : "\n") + ("[life] " + instance_ + ": " + w);

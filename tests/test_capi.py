@@ -157,3 +157,19 @@ def test_every_entry_point_rejects_null_arguments():
             fn.restype = ctypes.c_char_p
             assert isinstance(fn(*args), bytes), name
     assert checked >= 60
+
+
+def test_inspect_reports_the_direct_radius_limit_like_setup():
+    # The direct path holds R <= 32 (per kernel for directMulti); inspection
+    # (setup's host half) rejects what setup would, the spectral path not.
+    with pytest.raises(lb.LeniaError, match="status -2"):
+        lb.inspect({"radius": 40}, 256, 256)
+    assert lb.inspect({"radius": 32}, 256, 256)["status"] == 0
+    two = [{"radiusScale": 1.0}, {"radiusScale": 2.0}]
+    with pytest.raises(lb.LeniaError, match="kernel radius <= 32"):
+        lb.inspect({"radius": 20, "convMode": "directMulti", "kernels": two}, 256, 256)
+    assert lb.inspect({"radius": 16, "convMode": "directMulti", "kernels": two}, 256, 256)["radius"] == 16
+    assert lb.inspect({"radius": 40, "convMode": "fft"}, 256, 256)["conv_mode"] == lb.CONV_FFT
+    # A non-power-of-two size falls back to direct, where R = 40 is refused.
+    with pytest.raises(lb.LeniaError, match="radius <= 32"):
+        lb.inspect({"radius": 40, "convMode": "fft"}, 250, 256)
