@@ -127,3 +127,41 @@ def test_ref32_matches_compiled_reference_live():
         o.reset(trial)
         for f in range(3):
             np.testing.assert_array_equal(o.encode(f, 2, f + 5), r.encode(f, 2, f + 5))
+
+
+def test_reference_fft_roundtrip_within_its_stated_bound():
+    # The reference's own FFT check: a random 256x128 real field, forward
+    # then inverse, max abs error < 1e-4 (Shaders/Common/FFT.metal:29-34,
+    # docs/specs/phase9_lenia_fft.md:155-158). The forward transform is the
+    # unscaled DFT with exp(-i...) (numpy's convention).
+    rng = np.random.default_rng(11)
+    re = rng.random((128, 256)).astype(np.float32)
+    im = np.zeros_like(re)
+    fr, fi = lo.fft2d_ref_f32(re, im, +1)
+    want = np.fft.fft2(re.astype(np.float64))
+    scale = np.abs(want).max()
+    assert np.abs(fr - want.real).max() / scale < 1e-5
+    assert np.abs(fi - want.imag).max() / scale < 1e-5
+    rr, ri = lo.fft2d_ref_f32(fr, fi, -1)
+    assert np.abs(rr - re).max() < 1e-4
+    assert np.abs(ri).max() < 1e-4
+
+
+def test_reference_direct_and_fft_agree_after_one_step():
+    # The reference's convolution check: the same init and kernel (R=13) one
+    # step by convMode direct and by fft at 256x256, max abs difference
+    # < 1e-3 (docs/specs/phase9_lenia_fft.md:159-162); here on the FP32
+    # restatement of both paths.
+    rng = np.random.default_rng(5)
+    init = np.zeros((256, 256), np.float32)
+    init[96:160, 96:160] = rng.random((64, 64)).astype(np.float32)
+    out = {}
+    for conv in ("direct", "fft"):
+        o = OracleLenia({"radius": 13, "convMode": conv}, 256, 256, "ref32")
+        assert o.use_fft == (conv == "fft")
+        o.reset(1)
+        o.set_initial_field(init)
+        out[conv] = o.encode(0, 1)
+    d = np.abs(out["direct"].astype(np.float64) - out["fft"]).max()
+    assert 0.0 < d < 1e-3, d
+    assert np.abs(out["direct"] - init).max() > 1e-3  # the step changed the field
