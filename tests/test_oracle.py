@@ -5,7 +5,12 @@
   against the compiled reference live where oracle/_ref was built.
 * FP64 oracle vs FP32 restatement: close (the restatement's rounding only).
 * FP64 convolution two ways (numpy FFT vs tap-by-tap C): 1e-12.
+* The reference's stated checks: its FFT round trip, direct vs FFT after one
+  step, and the Orbium preset surviving 400 frames.
 """
+import json
+import os
+
 import numpy as np
 import pytest
 
@@ -165,3 +170,31 @@ def test_reference_direct_and_fft_agree_after_one_step():
     d = np.abs(out["direct"].astype(np.float64) - out["fft"]).max()
     assert 0.0 < d < 1e-3, d
     assert np.abs(out["direct"] - init).max() > 1e-3  # the step changed the field
+
+
+def test_orbium_glides_and_survives_400_frames():
+    # The reference's qualitative known answer: the Orbium preset
+    # (Presets/lenia_orbium.json, stamp init of Presets/organisms/orbium.json
+    # with its own R, T, mu, sigma) survives 400 frames as a glider
+    # (docs/specs/phase11_organisms.md:74-81). One stamp on a 96x96 torus,
+    # FP32 restatement: the mass holds and the pattern moves.
+    ref = "/root/reference"
+    preset = os.path.join(ref, "Presets", "lenia_orbium.json")
+    if not os.path.exists(preset):
+        pytest.skip("reference presets not present")
+    params = json.load(open(preset))["modules"][0]["params"]
+    d = json.load(open(os.path.join(ref, params["organism"])))
+    org = lo.Organism(np.asarray(d["cells"], np.float32), d["R"], d["T"], d["mu"], d["sigma"])
+    p = dict(params, simWidth=96, simHeight=96, stampCount=1, stampRotate=False)
+    o = OracleLenia(p, 96, 96, "ref32", organism=org)
+    o.reset(7777)
+    first = o.encode(0, 1)
+    m0 = float(first.sum())
+    assert m0 > 10.0
+    for fr in range(1, 400):
+        f = o.encode(fr, 1)
+        if fr % 50 == 49:
+            assert 0.8 * m0 < float(f.sum()) < 1.2 * m0, (fr, float(f.sum()), m0)
+            assert f.max() > 0.5
+    body0, body = first > 0.1, f > 0.1
+    assert (body0 & body).sum() < 0.25 * body0.sum()  # it has moved off its start
