@@ -1,6 +1,6 @@
 /* oracle/lenia_oracle.c -- CPU oracle for the Lenia field update.
  *
- * TEST INFRASTRUCTURE ONLY (see lenia_oracle.h): the checker the CUDA path is
+ * TEST INFRASTRUCTURE ONLY (see lenia_oracle.h): the oracle the CUDA path is
  * compared against, never part of the product. Reference citations are
  * file:line within daitomanabe/life-simulation.
  */
