@@ -339,8 +339,11 @@ const char* lenia_batch_last_message(lenia_batch* b);
  *
  * field_in, field_out: distinct, 16-byte aligned device buffers of height x
  *   width floats.
- * cfg: kernels, num_kernels (0: one kernel from fp's growth mu/sigma),
- *   radius, kernel_shell_sigma, kernel_core; its other fields are unused.
+ * cfg: kernels, num_kernels (0: one kernel from fp's growth mu/sigma; more
+ *   than 4: the first 4, as the module's setup truncates), radius,
+ *   kernel_shell_sigma, kernel_core; its other fields are unused. A zero
+ *   sigma (a kernel's, or fp->growth_sigma when num_kernels is 0) is
+ *   LENIA_ERR_INVALID_ARG.
  * fp: the per-frame values; seed: the substep seed (the module uses
  *   pcgHash(deriveSeed(reset_seed) ^ (frame_index*197 + substep))).
  * Sizes: even width, width/2 and height with prime factors 2, 3, 5 only, and
@@ -352,7 +355,11 @@ const char* lenia_batch_last_message(lenia_batch* b);
  * them into the array synchronously on `stream`; other calls only queue
  * kernels on `stream`. All calls share the one array and each call fully
  * rewrites the parts it reads, so nothing needs clearing, but calls that
- * overlap on the GPU (other streams or host threads) race on it. */
+ * overlap on the GPU (other streams or host threads) race on it. A
+ * cudaDeviceReset discards the array with the context; calls after one are
+ * not supported (the tables are rebuilt only if the array's device address
+ * changed). Host-side failures, an allocation of the host tables included,
+ * return a status; no C++ exception leaves the call. */
 #define LENIA_NOALLOC_SCRATCH_BYTES (8u * 1024u * 1024u)
 int lenia_fft_step_noalloc(const float* field_in, float* field_out, uint32_t width, uint32_t height,
                            const lenia_config* cfg, const lenia_frame_params* fp, uint32_t seed,

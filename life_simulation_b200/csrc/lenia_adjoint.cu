@@ -33,10 +33,12 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <memory>
 #include <string>
 #include <vector>
 
 #include "../../include/lenia_b200.h"
+#include "abi_guard.h"
 #include "fft_fast_common.cuh"
 #include "lenia_device.cuh"
 #include "lenia_kernels.h"
@@ -1018,171 +1020,183 @@ cudaError_t autotune(lenia_adjoint* a) {
 extern "C" {
 
 int lenia_adjoint_create(const lenia_adjoint_config* cfg, lenia_adjoint** out) {
-    using namespace lenia;
-    if (!cfg || !out) return LENIA_ERR_INVALID_ARG;
-    *out = nullptr;
-    auto* a = new lenia_adjoint();
-    const auto bail = [&](int code) {
-        g_adjoint_create_error = a->message;
-        delete a;
-        return code;
-    };
-    a->cfg = *cfg;
-    std::string why;
-    if (check_kernels(cfg->kernels, cfg->num_kernels, why) != LENIA_OK) return bail(a->fail(LENIA_ERR_INVALID_ARG, why));
-    if (cfg->batch < 1 || cfg->steps < 1 || cfg->checkpoint_every < 1 || cfg->checkpoint_every > cfg->steps)
-        return bail(a->fail(LENIA_ERR_INVALID_ARG, "need batch >= 1, steps >= 1, 1 <= checkpoint_every <= steps"));
-    if (cfg->radius < 1 || cfg->growth_mode > 1u || cfg->kernel_core > 1u || !std::isfinite(cfg->dt))
-        return bail(a->fail(LENIA_ERR_INVALID_ARG, "radius >= 1, growth_mode 0/1, kernel_core 0/1, finite dt"));
-    if (cfg->kernel_core == LENIA_CORE_GAUSS_SHELL && !(cfg->shell_sigma > 0.0f))
-        return bail(a->fail(LENIA_ERR_INVALID_ARG, "shell_sigma must be positive"));
-    FastPlan cf, ri;
-    if (cfg->width % 2 || cfg->width / 2 % kSpectralBlock || !fast_col_plan(int(cfg->height), cf) ||
-        !fast_row_plan(int(cfg->width / 2), ri))
-        return bail(a->fail(LENIA_ERR_UNSUPPORTED, "field size " + std::to_string(cfg->width) + "x" +
-                                                       std::to_string(cfg->height) +
-                                                       " has no compile-time FFT plan"));
-    a->W = int(cfg->width);
-    a->H = int(cfg->height);
-    a->M = a->W / 2;
-    a->Hh = a->H / 2 + 1;
-    a->nb = int(cfg->batch);
-    a->nk = int(cfg->num_kernels);
-    a->T = int(cfg->steps);
-    a->C = int(cfg->checkpoint_every);
-    a->nck = (a->T + a->C - 1) / a->C + 1;
-    a->P = size_t(a->W) * a->H;
-    a->SPX = size_t(a->M) * a->H;
-    cudaGetDevice(&a->device);
-    cudaError_t e = cudaStreamCreateWithFlags(&a->stream, cudaStreamNonBlocking);
-    if (e != cudaSuccess) return bail(a->cuda_fail(e, "cudaStreamCreate"));
-    const size_t nb = size_t(a->nb), nk = size_t(a->nk);
-    int ntab = 0;
-    for (int k = 0; k < a->nk; ++k)
-        if (cfg->kernels[k].num_betas > 1) ntab += int(cfg->kernels[k].num_betas);
-    const size_t tab = size_t(a->M + 1) * a->Hh;
-    if ((e = a->alloc(&a->ckpt, size_t(a->nck) * nb * a->P)) != cudaSuccess ||
-        (e = a->alloc(&a->seg, size_t(a->C) * nb * a->P)) != cudaSuccess ||
-        (e = a->alloc(&a->Sring, size_t(a->C + 1) * nb * a->SPX)) != cudaSuccess ||
-        (e = a->alloc(&a->Uspec, nb * nk * a->SPX)) != cudaSuccess ||
-        (e = a->alloc(&a->Upx, size_t(a->C) * nb * nk * a->P)) != cudaSuccess ||
-        (e = a->alloc(&a->SQ, nb * nk * a->SPX)) != cudaSuccess || (e = a->alloc(&a->SG, nb * a->SPX)) != cudaSuccess ||
-        (e = a->alloc(&a->g[0], nb * a->P)) != cudaSuccess || (e = a->alloc(&a->g[1], nb * a->P)) != cudaSuccess ||
-        (e = a->alloc(&a->gio, nb * a->P)) != cudaSuccess || (e = a->alloc(&a->acc, size_t(kAcc))) != cudaSuccess ||
-        (e = a->alloc(&a->khat, nk * tab)) != cudaSuccess ||
-        (e = a->alloc(&a->dtab, std::max<size_t>(1, size_t(ntab)) * tab)) != cudaSuccess ||
-        (e = a->alloc(&a->d_r2c, size_t(a->nck - 1) * nb)) != cudaSuccess ||
-        (e = a->alloc(&a->d_fcol, size_t(a->T) * nb)) != cudaSuccess ||
-        (e = a->alloc(&a->d_frow, size_t(a->T) * nb)) != cudaSuccess ||
-        (e = a->alloc(&a->d_ffwd, size_t(a->T) * nb)) != cudaSuccess ||
-        (e = a->alloc(&a->d_arow, size_t(a->T + 1) * nb)) != cudaSuccess ||
-        (e = a->alloc(&a->d_acol, size_t(a->T) * nb)) != cudaSuccess)
-        return bail(a->cuda_fail(e, "cudaMalloc"));
-    std::vector<float2> t2;
-    fill_twiddles(a->W, t2);
-    t2.resize(size_t(a->M) + 1);
-    std::vector<float2> tws[4];
-    fast_twiddle_tables(a->H, a->M, tws);
-    if ((e = a->alloc(&a->tw_r2c, t2.size())) != cudaSuccess) return bail(a->cuda_fail(e, "cudaMalloc"));
-    cudaMemcpy(a->tw_r2c, t2.data(), t2.size() * sizeof(float2), cudaMemcpyHostToDevice);
-    for (int q = 0; q < 4; ++q) {
-        if ((e = a->alloc(&a->tw[q], tws[q].size())) != cudaSuccess) return bail(a->cuda_fail(e, "cudaMalloc"));
-        cudaMemcpy(a->tw[q], tws[q].data(), tws[q].size() * sizeof(float2), cudaMemcpyHostToDevice);
-    }
-    a->ft.col_twf = a->tw[0];
-    a->ft.col_twi = a->tw[1];
-    a->ft.row_twi = a->tw[2];
-    a->ft.row_twf = a->tw[3];
-    int rc = a->set_kernels(cfg->kernels, cfg->num_kernels, cfg->dt);
-    if (rc != LENIA_OK) return bail(rc);
-    if ((e = autotune(a)) != cudaSuccess) return bail(a->cuda_fail(e, "autotune"));
-    if ((e = cudaDeviceSynchronize()) != cudaSuccess) return bail(a->cuda_fail(e, "setup"));
-    *out = a;
-    return LENIA_OK;
+    return lenia::abi_guard(&g_adjoint_create_error, [&]() -> int {
+        using namespace lenia;
+        if (!cfg || !out) return LENIA_ERR_INVALID_ARG;
+        *out = nullptr;
+        std::unique_ptr<lenia_adjoint> holder(new lenia_adjoint());
+        lenia_adjoint* a = holder.get();
+        const auto bail = [&](int code) {
+            g_adjoint_create_error = a->message;
+            return code;  // the holder frees the half-built engine
+        };
+        a->cfg = *cfg;
+        std::string why;
+        if (check_kernels(cfg->kernels, cfg->num_kernels, why) != LENIA_OK) return bail(a->fail(LENIA_ERR_INVALID_ARG, why));
+        if (cfg->batch < 1 || cfg->steps < 1 || cfg->checkpoint_every < 1 || cfg->checkpoint_every > cfg->steps)
+            return bail(a->fail(LENIA_ERR_INVALID_ARG, "need batch >= 1, steps >= 1, 1 <= checkpoint_every <= steps"));
+        if (cfg->radius < 1 || cfg->growth_mode > 1u || cfg->kernel_core > 1u || !std::isfinite(cfg->dt))
+            return bail(a->fail(LENIA_ERR_INVALID_ARG, "radius >= 1, growth_mode 0/1, kernel_core 0/1, finite dt"));
+        if (cfg->kernel_core == LENIA_CORE_GAUSS_SHELL && !(cfg->shell_sigma > 0.0f))
+            return bail(a->fail(LENIA_ERR_INVALID_ARG, "shell_sigma must be positive"));
+        FastPlan cf, ri;
+        if (cfg->width % 2 || cfg->width / 2 % kSpectralBlock || !fast_col_plan(int(cfg->height), cf) ||
+            !fast_row_plan(int(cfg->width / 2), ri))
+            return bail(a->fail(LENIA_ERR_UNSUPPORTED, "field size " + std::to_string(cfg->width) + "x" +
+                                                           std::to_string(cfg->height) +
+                                                           " has no compile-time FFT plan"));
+        a->W = int(cfg->width);
+        a->H = int(cfg->height);
+        a->M = a->W / 2;
+        a->Hh = a->H / 2 + 1;
+        a->nb = int(cfg->batch);
+        a->nk = int(cfg->num_kernels);
+        a->T = int(cfg->steps);
+        a->C = int(cfg->checkpoint_every);
+        a->nck = (a->T + a->C - 1) / a->C + 1;
+        a->P = size_t(a->W) * a->H;
+        a->SPX = size_t(a->M) * a->H;
+        cudaGetDevice(&a->device);
+        cudaError_t e = cudaStreamCreateWithFlags(&a->stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) return bail(a->cuda_fail(e, "cudaStreamCreate"));
+        const size_t nb = size_t(a->nb), nk = size_t(a->nk);
+        int ntab = 0;
+        for (int k = 0; k < a->nk; ++k)
+            if (cfg->kernels[k].num_betas > 1) ntab += int(cfg->kernels[k].num_betas);
+        const size_t tab = size_t(a->M + 1) * a->Hh;
+        if ((e = a->alloc(&a->ckpt, size_t(a->nck) * nb * a->P)) != cudaSuccess ||
+            (e = a->alloc(&a->seg, size_t(a->C) * nb * a->P)) != cudaSuccess ||
+            (e = a->alloc(&a->Sring, size_t(a->C + 1) * nb * a->SPX)) != cudaSuccess ||
+            (e = a->alloc(&a->Uspec, nb * nk * a->SPX)) != cudaSuccess ||
+            (e = a->alloc(&a->Upx, size_t(a->C) * nb * nk * a->P)) != cudaSuccess ||
+            (e = a->alloc(&a->SQ, nb * nk * a->SPX)) != cudaSuccess || (e = a->alloc(&a->SG, nb * a->SPX)) != cudaSuccess ||
+            (e = a->alloc(&a->g[0], nb * a->P)) != cudaSuccess || (e = a->alloc(&a->g[1], nb * a->P)) != cudaSuccess ||
+            (e = a->alloc(&a->gio, nb * a->P)) != cudaSuccess || (e = a->alloc(&a->acc, size_t(kAcc))) != cudaSuccess ||
+            (e = a->alloc(&a->khat, nk * tab)) != cudaSuccess ||
+            (e = a->alloc(&a->dtab, std::max<size_t>(1, size_t(ntab)) * tab)) != cudaSuccess ||
+            (e = a->alloc(&a->d_r2c, size_t(a->nck - 1) * nb)) != cudaSuccess ||
+            (e = a->alloc(&a->d_fcol, size_t(a->T) * nb)) != cudaSuccess ||
+            (e = a->alloc(&a->d_frow, size_t(a->T) * nb)) != cudaSuccess ||
+            (e = a->alloc(&a->d_ffwd, size_t(a->T) * nb)) != cudaSuccess ||
+            (e = a->alloc(&a->d_arow, size_t(a->T + 1) * nb)) != cudaSuccess ||
+            (e = a->alloc(&a->d_acol, size_t(a->T) * nb)) != cudaSuccess)
+            return bail(a->cuda_fail(e, "cudaMalloc"));
+        std::vector<float2> t2;
+        fill_twiddles(a->W, t2);
+        t2.resize(size_t(a->M) + 1);
+        std::vector<float2> tws[4];
+        fast_twiddle_tables(a->H, a->M, tws);
+        if ((e = a->alloc(&a->tw_r2c, t2.size())) != cudaSuccess) return bail(a->cuda_fail(e, "cudaMalloc"));
+        cudaMemcpy(a->tw_r2c, t2.data(), t2.size() * sizeof(float2), cudaMemcpyHostToDevice);
+        for (int q = 0; q < 4; ++q) {
+            if ((e = a->alloc(&a->tw[q], tws[q].size())) != cudaSuccess) return bail(a->cuda_fail(e, "cudaMalloc"));
+            cudaMemcpy(a->tw[q], tws[q].data(), tws[q].size() * sizeof(float2), cudaMemcpyHostToDevice);
+        }
+        a->ft.col_twf = a->tw[0];
+        a->ft.col_twi = a->tw[1];
+        a->ft.row_twi = a->tw[2];
+        a->ft.row_twf = a->tw[3];
+        int rc = a->set_kernels(cfg->kernels, cfg->num_kernels, cfg->dt);
+        if (rc != LENIA_OK) return bail(rc);
+        if ((e = autotune(a)) != cudaSuccess) return bail(a->cuda_fail(e, "autotune"));
+        if ((e = cudaDeviceSynchronize()) != cudaSuccess) return bail(a->cuda_fail(e, "setup"));
+        *out = holder.release();
+        return LENIA_OK;
+    });
 }
 
 int lenia_adjoint_destroy(lenia_adjoint* a) {
-    if (!a) return LENIA_ERR_INVALID_ARG;
-    delete a;
-    return LENIA_OK;
+    return lenia::abi_guard(a ? &a->message : nullptr, [&]() -> int {
+        if (!a) return LENIA_ERR_INVALID_ARG;
+        delete a;
+        return LENIA_OK;
+    });
 }
 
 int lenia_adjoint_set_params(lenia_adjoint* a, const lenia_kernel_def* kernels, uint32_t num_kernels, float dt) {
-    if (!a || !kernels) return LENIA_ERR_INVALID_ARG;
-    std::string why;
-    if (check_kernels(kernels, num_kernels, why) != LENIA_OK) return a->fail(LENIA_ERR_INVALID_ARG, why);
-    if (int(num_kernels) != a->nk) return a->fail(LENIA_ERR_INVALID_ARG, "num_kernels differs from creation");
-    for (int k = 0; k < a->nk; ++k) {
-        if (kernels[k].num_betas != a->cfg.kernels[k].num_betas)
-            return a->fail(LENIA_ERR_INVALID_ARG, "num_betas of a kernel differs from creation");
-        if (kernels[k].radius_scale != a->cfg.kernels[k].radius_scale)
-            return a->fail(LENIA_ERR_INVALID_ARG, "radius_scale of a kernel differs from creation");
-    }
-    if (!std::isfinite(dt)) return a->fail(LENIA_ERR_INVALID_ARG, "dt must be finite");
-    // The tables are read by queued launches (on any stream): wait first.
-    cudaDeviceSynchronize();
-    return a->set_kernels(kernels, num_kernels, dt);
+    return lenia::abi_guard(a ? &a->message : nullptr, [&]() -> int {
+        if (!a || !kernels) return LENIA_ERR_INVALID_ARG;
+        std::string why;
+        if (check_kernels(kernels, num_kernels, why) != LENIA_OK) return a->fail(LENIA_ERR_INVALID_ARG, why);
+        if (int(num_kernels) != a->nk) return a->fail(LENIA_ERR_INVALID_ARG, "num_kernels differs from creation");
+        for (int k = 0; k < a->nk; ++k) {
+            if (kernels[k].num_betas != a->cfg.kernels[k].num_betas)
+                return a->fail(LENIA_ERR_INVALID_ARG, "num_betas of a kernel differs from creation");
+            if (kernels[k].radius_scale != a->cfg.kernels[k].radius_scale)
+                return a->fail(LENIA_ERR_INVALID_ARG, "radius_scale of a kernel differs from creation");
+        }
+        if (!std::isfinite(dt)) return a->fail(LENIA_ERR_INVALID_ARG, "dt must be finite");
+        // The tables are read by queued launches (on any stream): wait first.
+        cudaDeviceSynchronize();
+        return a->set_kernels(kernels, num_kernels, dt);
+    });
 }
 
 int lenia_adjoint_forward(lenia_adjoint* a, const float* a0, float* a_final, void* stream) {
-    if (!a || !a0 || !a_final) return LENIA_ERR_INVALID_ARG;
-    const cudaStream_t s = pick_stream(a, stream);
-    const size_t n = size_t(a->nb) * a->P * sizeof(float);
-    cudaError_t e = cudaMemcpyAsync(a->ckpt, a0, n, cudaMemcpyDeviceToDevice, s);
-    if (e == cudaSuccess) e = row_spectrum(a, 0, s);
-    for (int t = 0; t < a->T && e == cudaSuccess; ++t) e = forward_step(a, t, false, s);
-    if (e == cudaSuccess)
-        e = cudaMemcpyAsync(a_final, a->slot(a->T, 0), n, cudaMemcpyDeviceToDevice, s);
-    if (e != cudaSuccess) return a->cuda_fail(e, "forward");
-    a->forward_done = true;
-    a->last_segment_fresh = true;
-    return LENIA_OK;
+    return lenia::abi_guard(a ? &a->message : nullptr, [&]() -> int {
+        if (!a || !a0 || !a_final) return LENIA_ERR_INVALID_ARG;
+        const cudaStream_t s = pick_stream(a, stream);
+        const size_t n = size_t(a->nb) * a->P * sizeof(float);
+        cudaError_t e = cudaMemcpyAsync(a->ckpt, a0, n, cudaMemcpyDeviceToDevice, s);
+        if (e == cudaSuccess) e = row_spectrum(a, 0, s);
+        for (int t = 0; t < a->T && e == cudaSuccess; ++t) e = forward_step(a, t, false, s);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(a_final, a->slot(a->T, 0), n, cudaMemcpyDeviceToDevice, s);
+        if (e != cudaSuccess) return a->cuda_fail(e, "forward");
+        a->forward_done = true;
+        a->last_segment_fresh = true;
+        return LENIA_OK;
+    });
 }
 
 int lenia_adjoint_backward(lenia_adjoint* a, const float* g_final, float* g_initial, double* grad_params,
                            void* stream) {
-    using namespace lenia;
-    if (!a || !g_final || !g_initial) return LENIA_ERR_INVALID_ARG;
-    if (!a->forward_done) return a->fail(LENIA_ERR_STATE, "backward needs a forward with the current parameters");
-    const cudaStream_t s = pick_stream(a, stream);
-    const size_t n = size_t(a->nb) * a->P * sizeof(float);
-    cudaError_t e = cudaMemsetAsync(a->acc, 0, sizeof(double) * kAcc, s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(a->gio, g_final, n, cudaMemcpyDeviceToDevice, s);
-    for (int j = a->nck - 2; j >= 0 && e == cudaSuccess; --j) {
-        const int s0 = j * a->C, e0 = std::min(s0 + a->C, a->T);
-        if (!(j == a->nck - 2 && a->last_segment_fresh)) {
-            e = row_spectrum(a, j, s);
-            for (int t = s0; t < e0 && e == cudaSuccess; ++t) e = forward_step(a, t, true, s);
+    return lenia::abi_guard(a ? &a->message : nullptr, [&]() -> int {
+        using namespace lenia;
+        if (!a || !g_final || !g_initial) return LENIA_ERR_INVALID_ARG;
+        if (!a->forward_done) return a->fail(LENIA_ERR_STATE, "backward needs a forward with the current parameters");
+        const cudaStream_t s = pick_stream(a, stream);
+        const size_t n = size_t(a->nb) * a->P * sizeof(float);
+        cudaError_t e = cudaMemsetAsync(a->acc, 0, sizeof(double) * kAcc, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(a->gio, g_final, n, cudaMemcpyDeviceToDevice, s);
+        for (int j = a->nck - 2; j >= 0 && e == cudaSuccess; --j) {
+            const int s0 = j * a->C, e0 = std::min(s0 + a->C, a->T);
+            if (!(j == a->nck - 2 && a->last_segment_fresh)) {
+                e = row_spectrum(a, j, s);
+                for (int t = s0; t < e0 && e == cudaSuccess; ++t) e = forward_step(a, t, true, s);
+            }
+            for (int t = e0 - 1; t >= s0 && e == cudaSuccess; --t) {
+                e = launch_row_adj(a->M, a->adj_row_batch, a->d_arow + size_t(t) * a->nb, a->nb, a->rargs, a->tw_r2c,
+                                   a->ft, s);
+                if (e == cudaSuccess)
+                    e = launch_col_adj(a->H, a->adj_col_batch, a->d_acol + size_t(t) * a->nb, a->nb, a->cargs, a->ft, s);
+                a->launches += 2;
+            }
         }
-        for (int t = e0 - 1; t >= s0 && e == cudaSuccess; --t) {
-            e = launch_row_adj(a->M, a->adj_row_batch, a->d_arow + size_t(t) * a->nb, a->nb, a->rargs, a->tw_r2c,
+        if (e == cudaSuccess) {
+            e = launch_row_adj(a->M, a->adj_row_batch, a->d_arow + size_t(a->T) * a->nb, a->nb, a->rargs, a->tw_r2c,
                                a->ft, s);
-            if (e == cudaSuccess)
-                e = launch_col_adj(a->H, a->adj_col_batch, a->d_acol + size_t(t) * a->nb, a->nb, a->cargs, a->ft, s);
-            a->launches += 2;
+            a->launches += 1;
         }
-    }
-    if (e == cudaSuccess) {
-        e = launch_row_adj(a->M, a->adj_row_batch, a->d_arow + size_t(a->T) * a->nb, a->nb, a->rargs, a->tw_r2c,
-                           a->ft, s);
-        a->launches += 1;
-    }
-    if (e == cudaSuccess) e = cudaMemcpyAsync(g_initial, a->gio, n, cudaMemcpyDeviceToDevice, s);
-    if (e == cudaSuccess && grad_params) {
-        finalize_kernel<<<1, 64, 0, s>>>(a->acc, grad_params, a->nk, a->cfg.growth_mode == 1u ? 1 : 0);
-        e = cudaGetLastError();
-        a->launches += 1;
-    }
-    a->last_segment_fresh = false;
-    if (e != cudaSuccess) return a->cuda_fail(e, "backward");
-    return LENIA_OK;
+        if (e == cudaSuccess) e = cudaMemcpyAsync(g_initial, a->gio, n, cudaMemcpyDeviceToDevice, s);
+        if (e == cudaSuccess && grad_params) {
+            finalize_kernel<<<1, 64, 0, s>>>(a->acc, grad_params, a->nk, a->cfg.growth_mode == 1u ? 1 : 0);
+            e = cudaGetLastError();
+            a->launches += 1;
+        }
+        a->last_segment_fresh = false;
+        if (e != cudaSuccess) return a->cuda_fail(e, "backward");
+        return LENIA_OK;
+    });
 }
 
 int lenia_adjoint_stats(lenia_adjoint* a, uint64_t* device_bytes, uint64_t* launches) {
-    if (!a) return LENIA_ERR_INVALID_ARG;
-    if (device_bytes) *device_bytes = a->bytes;
-    if (launches) *launches = a->launches;
-    return LENIA_OK;
+    return lenia::abi_guard(a ? &a->message : nullptr, [&]() -> int {
+        if (!a) return LENIA_ERR_INVALID_ARG;
+        if (device_bytes) *device_bytes = a->bytes;
+        if (launches) *launches = a->launches;
+        return LENIA_OK;
+    });
 }
 
 // NULL: the calling thread's last failed lenia_adjoint_create.

@@ -26,6 +26,7 @@
 #include <vector>
 
 #include "../../include/lenia_b200.h"
+#include "abi_guard.h"
 #include "colormap.cuh"
 #include "lenia_device.cuh"
 #include "lenia_kernels.h"
@@ -232,561 +233,594 @@ struct lenia_batch {
 
 using lenia::BatchContext;
 
+namespace {
+// Message of the calling thread's last failed lenia_batch_create.
+thread_local std::string g_batch_create_error;
+}  // namespace
+
 extern "C" {
 
 int lenia_batch_create(const lenia_world* worlds, uint32_t n, uint32_t policy, lenia_batch** out) {
-    using namespace lenia;
-    if (!worlds || !out || n == 0) return LENIA_ERR_INVALID_ARG;
-    *out = nullptr;
-    auto holder = std::make_unique<lenia_batch>();
-    BatchContext& b = holder->ctx;
-    b.worlds.assign(worlds, worlds + n);
-    if (cudaGetDevice(&b.device) != cudaSuccess) return LENIA_ERR_NO_DEVICE;
-    cudaError_t e = cudaStreamCreateWithFlags(&b.stream, cudaStreamNonBlocking);
-    if (e != cudaSuccess) return LENIA_ERR_CUDA;
+    g_batch_create_error.clear();
+    std::unique_ptr<lenia_batch> holder;
+    const int rc = lenia::abi_guard(&g_batch_create_error, [&]() -> int {
+        using namespace lenia;
+        if (!worlds || !out || n == 0) return LENIA_ERR_INVALID_ARG;
+        *out = nullptr;
+        holder = std::make_unique<lenia_batch>();
+        BatchContext& b = holder->ctx;
+        b.worlds.assign(worlds, worlds + n);
+        if (cudaGetDevice(&b.device) != cudaSuccess) return LENIA_ERR_NO_DEVICE;
+        cudaError_t e = cudaStreamCreateWithFlags(&b.stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) return LENIA_ERR_CUDA;
 
-    // Fields.
-    size_t total = 0;
-    b.field_off.resize(n);
-    for (uint32_t i = 0; i < n; ++i) {
-        const lenia_world& w = worlds[i];
-        if (w.width < 1 || w.height < 1 || !(w.sigma != 0.0f)) return LENIA_ERR_INVALID_ARG;
-        if (w.radius > uint32_t(kMaxRadius) && (w.width % 2 || w.width < 2)) return LENIA_ERR_UNSUPPORTED;
-        b.field_off[i] = total;
-        total += 2 * size_t(w.width) * w.height;
-    }
-    if ((e = b.alloc(&b.fields, total)) != cudaSuccess) return LENIA_ERR_CUDA;
-    cudaMemsetAsync(b.fields, 0, total * sizeof(float), b.stream);
+        // Fields.
+        size_t total = 0;
+        b.field_off.resize(n);
+        for (uint32_t i = 0; i < n; ++i) {
+            const lenia_world& w = worlds[i];
+            if (w.width < 1 || w.height < 1 || !(w.sigma != 0.0f)) return LENIA_ERR_INVALID_ARG;
+            if (w.radius > uint32_t(kMaxRadius) && (w.width % 2 || w.width < 2)) return LENIA_ERR_UNSUPPORTED;
+            b.field_off[i] = total;
+            total += 2 * size_t(w.width) * w.height;
+        }
+        if ((e = b.alloc(&b.fields, total)) != cudaSuccess) return LENIA_ERR_CUDA;
+        cudaMemsetAsync(b.fields, 0, total * sizeof(float), b.stream);
 
-    // Which worlds can take which path.
-    std::vector<bool> can_fft(n), can_direct(n);
-    for (uint32_t i = 0; i < n; ++i) {
-        const lenia_world& w = worlds[i];
-        FastPlan cf, ri;
-        can_fft[i] = w.width % 2 == 0 && fast_col_plan(int(w.height), cf) && fast_row_plan(int(w.width / 2), ri) &&
-                     (w.width / 2) % kSpectralBlock == 0;
-        can_direct[i] = w.radius <= uint32_t(kMaxRadius);
-        if (!can_fft[i] && !can_direct[i]) {
-            b.message = "world " + std::to_string(i) + ": radius > 32 needs a spectral size (see fast plans)";
-            return LENIA_ERR_UNSUPPORTED;
-        }
-    }
-    b.path.assign(n, LENIA_CONV_DIRECT);
-    for (uint32_t i = 0; i < n; ++i) {
-        if (policy == LENIA_BATCH_FFT && !can_fft[i]) return LENIA_ERR_UNSUPPORTED;
-        if (policy == LENIA_BATCH_DIRECT && !can_direct[i]) return LENIA_ERR_UNSUPPORTED;
-        b.path[i] = (policy == LENIA_BATCH_FFT || !can_direct[i]) ? LENIA_CONV_FFT : LENIA_CONV_DIRECT;
-    }
-
-    // Direct LUTs for every world that might take the direct path.
-    std::vector<std::vector<float>> luts(n);
-    std::vector<uint32_t> nnz(n, 0);
-    for (uint32_t i = 0; i < n; ++i)
-        if (can_direct[i]) {
-            build_direct_lut(worlds[i].radius, worlds[i].shell_mu, worlds[i].shell_sigma, worlds[i].kernel_core,
-                             luts[i]);
-            nnz[i] = nnz_taps(luts[i]);
-        }
-
-    // Spectral classes for every world that might take the spectral path.
-    std::map<std::pair<int, int>, int> class_of;
-    std::vector<int> cls(n, -1);
-    for (uint32_t i = 0; i < n; ++i)
-        if (can_fft[i]) {
-            auto key = std::make_pair(int(worlds[i].width), int(worlds[i].height));
-            auto it = class_of.find(key);
-            if (it == class_of.end()) {
-                BatchContext::SizeClass c;
-                c.W = key.first;
-                c.H = key.second;
-                c.M = c.W / 2;
-                class_of[key] = int(b.classes.size());
-                b.classes.push_back(c);
-                it = class_of.find(key);
-            }
-            cls[i] = it->second;
-        }
-
-    // Per-world parameters and the substep seed base.
-    std::vector<StepParams> params(n);
-    std::vector<uint32_t> base_seed(n);
-    for (uint32_t i = 0; i < n; ++i) {
-        params[i] = world_params(worlds[i]);
-        base_seed[i] = derive_seed(worlds[i].seed, 0x4C454E31u);
-    }
-    std::vector<std::vector<int>> class_members(b.classes.size());
-    for (uint32_t i = 0; i < n; ++i)
-        if (cls[i] >= 0) class_members[size_t(cls[i])].push_back(int(i));
-
-    // Spectral resources of every candidate world of each size class.
-    for (size_t ci = 0; ci < b.classes.size(); ++ci) {
-        auto& c = b.classes[ci];
-        const int cnt = int(class_members[ci].size());
-        const size_t spec = size_t(c.M) * c.H;
-        const int Hh = c.H / 2 + 1;
-        if ((e = b.alloc(&c.S, spec * cnt)) != cudaSuccess) return LENIA_ERR_CUDA;
-        if ((e = b.alloc(&c.U, spec * cnt)) != cudaSuccess) return LENIA_ERR_CUDA;
-        if ((e = b.alloc(&c.khat, size_t(c.M + 1) * Hh * cnt)) != cudaSuccess) return LENIA_ERR_CUDA;
-        std::vector<float> kh(size_t(c.M + 1) * Hh * cnt), img, sp;
-        for (int k = 0; k < cnt; ++k) {
-            const lenia_world& w = worlds[class_members[ci][size_t(k)]];
-            build_ring_image(w.width, w.height, float(w.radius), w.shell_sigma, std::vector<float>{1.0f},
-                             w.kernel_core, img);
-            kernel_spectrum(img, w.width, w.height, sp);
-            std::copy(sp.begin(), sp.end(), kh.begin() + size_t(k) * (c.M + 1) * Hh);
-        }
-        cudaMemcpy(c.khat, kh.data(), kh.size() * sizeof(float), cudaMemcpyHostToDevice);
-        std::vector<float2> t2;
-        fill_twiddles(c.W, t2);
-        t2.resize(size_t(c.M) + 1);
-        if ((e = b.alloc(&c.tw_r2c, t2.size())) != cudaSuccess) return LENIA_ERR_CUDA;
-        cudaMemcpy(c.tw_r2c, t2.data(), t2.size() * sizeof(float2), cudaMemcpyHostToDevice);
-        FastPlan cf, ri;
-        fast_col_plan(c.H, cf);
-        fast_row_plan(c.M, ri);
-        FastPlan rcf = cf, rri = ri;
-        for (int i = 0; i < cf.np; ++i) rcf.radix[i] = cf.radix[cf.np - 1 - i];
-        for (int i = 0; i < ri.np; ++i) rri.radix[i] = ri.radix[ri.np - 1 - i];
-        const FastPlan* plans[4] = {&cf, &rcf, &ri, &rri};
-        for (int q = 0; q < 4; ++q) {
-            std::vector<float2> tw;
-            fast_plan_twiddles(*plans[q], tw);
-            if (tw.empty()) tw.push_back(make_float2(1.0f, 0.0f));
-            if ((e = b.alloc(&c.tw[q], tw.size())) != cudaSuccess) return LENIA_ERR_CUDA;
-            cudaMemcpy(c.tw[q], tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice);
-        }
-        c.t.col_twf = c.tw[0];
-        c.t.col_twi = c.tw[1];
-        c.t.row_twi = c.tw[2];
-        c.t.row_twf = c.tw[3];
-    }
-
-    std::vector<int> slot_of(n, 0);
-    // Direct tables for a set of worlds (both parities) and their tile list.
-    auto build_direct = [&](const std::vector<int>& ids, DirectWorld** dtab, int3** dtiles, int* ntiles,
-                            int* max_r) -> int {
-        std::vector<float> all_w;
-        std::vector<uint32_t> all_s;
-        std::vector<DirectWorld> tab;
-        std::vector<int3> tiles;
-        std::vector<std::pair<size_t, size_t>> offs;
-        *max_r = 0;
-        for (int i : ids) {
-            const int R = int(worlds[i].radius);
-            DirectGeometry g{R, 2 * R + 1, (R + 3) / 4 * 4, 0};
-            g.wp = 2 * g.xp + 8;
-            const size_t wo = all_w.size(), so = all_s.size();
-            all_w.resize(wo + size_t(g.ksize) * g.wp, 0.0f);
-            all_s.resize(so + size_t(g.ksize), 128u);
-            for (int dy = 0; dy < g.ksize; ++dy) {
-                int lo = 1 << 30, hi = -(1 << 30);
-                for (int dx = -R; dx <= R; ++dx) {
-                    const float v = luts[size_t(i)][size_t(dy) * g.ksize + size_t(dx + R)];
-                    all_w[wo + size_t(dy) * g.wp + size_t(dx + g.xp)] = v;
-                    if (v != 0.0f) { lo = std::min(lo, dx); hi = std::max(hi, dx); }
-                }
-                if (lo <= hi) {
-                    const int start = (lo >= 0) ? (lo / 4) * 4 : -((-lo + 3) / 4) * 4;
-                    all_s[so + size_t(dy)] = uint32_t(start + 128) | (uint32_t((hi - start + 1 + 7) / 8) << 16);
-                }
-            }
-            offs.push_back({wo, so});
-            DirectWorld dw{};
-            dw.g = g;
-            dw.p = params[size_t(i)];
-            slot_of[size_t(i)] = int(tab.size());
-            for (int ty = 0; ty < (int(worlds[i].height) + 15) / 16; ++ty)
-                for (int tx = 0; tx < (int(worlds[i].width) + 31) / 32; ++tx)
-                    tiles.push_back(make_int3(int(tab.size()), tx, ty));
-            tab.push_back(dw);
-            *max_r = std::max(*max_r, R);
-        }
-        *ntiles = int(tiles.size());
-        if (tab.empty()) return LENIA_OK;
-        float* dw = nullptr;
-        uint32_t* ds = nullptr;
-        if (b.alloc(&dw, all_w.size()) != cudaSuccess || b.alloc(&ds, all_s.size()) != cudaSuccess ||
-            b.alloc(dtiles, tiles.size()) != cudaSuccess || b.alloc(&dtab[0], tab.size()) != cudaSuccess ||
-            b.alloc(&dtab[1], tab.size()) != cudaSuccess)
-            return LENIA_ERR_CUDA;
-        cudaMemcpy(dw, all_w.data(), all_w.size() * sizeof(float), cudaMemcpyHostToDevice);
-        cudaMemcpy(ds, all_s.data(), all_s.size() * sizeof(uint32_t), cudaMemcpyHostToDevice);
-        cudaMemcpy(*dtiles, tiles.data(), tiles.size() * sizeof(int3), cudaMemcpyHostToDevice);
-        for (int par = 0; par < 2; ++par) {
-            std::vector<DirectWorld> t2 = tab;
-            for (size_t k = 0; k < t2.size(); ++k) {
-                t2[k].weights = dw + offs[k].first;
-                t2[k].spans = ds + offs[k].second;
-                t2[k].src = b.field(ids[k], par);
-                t2[k].dst = b.field(ids[k], par ^ 1);
-            }
-            cudaMemcpy(dtab[par], t2.data(), t2.size() * sizeof(DirectWorld), cudaMemcpyHostToDevice);
-        }
-        return LENIA_OK;
-    };
-    // Spectral tables of one class for a subset of its candidate worlds.
-    auto build_spectral = [&](size_t ci, const std::vector<int>& ids, SpectralWorld** stab, SpectralWorld** r2c) -> int {
-        auto& c = b.classes[ci];
-        const size_t spec = size_t(c.M) * c.H;
-        const int Hh = c.H / 2 + 1;
-        std::vector<SpectralWorld> steady[2], rt[2];
-        for (int wi : ids) {
-            const size_t k = size_t(std::find(class_members[ci].begin(), class_members[ci].end(), wi) -
-                                    class_members[ci].begin());
-            slot_of[size_t(wi)] = int(steady[0].size());
-            for (int par = 0; par < 2; ++par) {
-                SpectralWorld sw{};
-                sw.S = c.S + spec * k;
-                sw.U = c.U + spec * k;
-                sw.khat = c.khat + size_t(c.M + 1) * Hh * k;
-                sw.A = b.field(wi, par);
-                sw.A_out = b.field(wi, par ^ 1);
-                sw.S_next = c.S + spec * k;
-                sw.M = c.M;
-                sw.nk = 1;
-                sw.p = params[size_t(wi)];
-                steady[par].push_back(sw);
-                SpectralWorld r = sw;
-                r.nk = 0;  // row spectrum of A only
-                r.A_out = nullptr;
-                r.U = nullptr;
-                rt[par].push_back(r);
+        // Which worlds can take which path.
+        std::vector<bool> can_fft(n), can_direct(n);
+        for (uint32_t i = 0; i < n; ++i) {
+            const lenia_world& w = worlds[i];
+            FastPlan cf, ri;
+            can_fft[i] = w.width % 2 == 0 && fast_col_plan(int(w.height), cf) && fast_row_plan(int(w.width / 2), ri) &&
+                         (w.width / 2) % kSpectralBlock == 0;
+            can_direct[i] = w.radius <= uint32_t(kMaxRadius);
+            if (!can_fft[i] && !can_direct[i]) {
+                b.message = "world " + std::to_string(i) + ": radius > 32 needs a spectral size (see fast plans)";
+                return LENIA_ERR_UNSUPPORTED;
             }
         }
-        if (ids.empty()) return LENIA_OK;
-        for (int par = 0; par < 2; ++par) {
-            if (b.alloc(&stab[par], steady[par].size()) != cudaSuccess || b.alloc(&r2c[par], rt[par].size()) != cudaSuccess)
-                return LENIA_ERR_CUDA;
-            cudaMemcpy(stab[par], steady[par].data(), steady[par].size() * sizeof(SpectralWorld), cudaMemcpyHostToDevice);
-            cudaMemcpy(r2c[par], rt[par].data(), rt[par].size() * sizeof(SpectralWorld), cudaMemcpyHostToDevice);
+        b.path.assign(n, LENIA_CONV_DIRECT);
+        for (uint32_t i = 0; i < n; ++i) {
+            if (policy == LENIA_BATCH_FFT && !can_fft[i]) return LENIA_ERR_UNSUPPORTED;
+            if (policy == LENIA_BATCH_DIRECT && !can_direct[i]) return LENIA_ERR_UNSUPPORTED;
+            b.path[i] = (policy == LENIA_BATCH_FFT || !can_direct[i]) ? LENIA_CONV_FFT : LENIA_CONV_DIRECT;
         }
-        return LENIA_OK;
-    };
 
-    // Autotuner (policy AUTO): time the batched direct launch over every
-    // direct candidate (cost per pixel-tap) and each class's spectral step
-    // over all its candidates (cost per pixel) -- the batch's own launch
-    // shapes, on its own buffers -- and give each world the cheaper path.
-    if (policy == LENIA_BATCH_AUTO) {
-        cudaEvent_t ea, eb;
-        cudaEventCreate(&ea);
-        cudaEventCreate(&eb);
-        auto time_ms = [&](auto&& fn) {
-            float best = 1e30f;
-            for (int rep = 0; rep < 3; ++rep) {
-                cudaEventRecord(ea, b.stream);
-                if (fn() != cudaSuccess) return 1e30f;
-                cudaEventRecord(eb, b.stream);
-                cudaEventSynchronize(eb);
-                float ms = 0.0f;
-                cudaEventElapsedTime(&ms, ea, eb);
-                if (rep > 0) best = std::min(best, ms);
-            }
-            return best;
-        };
-        // Cost per tap of the batched direct launch over every candidate.
-        // That launch sizes its halo tile for the largest radius it holds,
-        // which overstates the cost for small radii; so candidates are also
-        // timed in radius bands, each with its own halo, and a band with
-        // enough work (>= 1e8 pixel-taps, so the launch itself is amortised)
-        // uses its own figure.
-        const auto band = [&](uint32_t i) { return worlds[i].radius <= 12u ? 0 : worlds[i].radius <= 20u ? 1 : 2; };
-        std::vector<int> dall, dcand[3];
-        double taps_all = 0.0, taps[3] = {0.0, 0.0, 0.0};
+        // Direct LUTs for every world that might take the direct path.
+        std::vector<std::vector<float>> luts(n);
+        std::vector<uint32_t> nnz(n, 0);
         for (uint32_t i = 0; i < n; ++i)
-            if (can_direct[i] && can_fft[i]) {
-                const double t = double(worlds[i].width) * worlds[i].height * nnz[i];
-                dall.push_back(int(i));
-                dcand[band(i)].push_back(int(i));
-                taps_all += t;
-                taps[band(i)] += t;
+            if (can_direct[i]) {
+                build_direct_lut(worlds[i].radius, worlds[i].shell_mu, worlds[i].shell_sigma, worlds[i].kernel_core,
+                                 luts[i]);
+                nnz[i] = nnz_taps(luts[i]);
             }
-        const auto time_direct = [&](const std::vector<int>& ids, double t, double& out) {
-            DirectWorld* dt[2] = {nullptr, nullptr};
-            int3* tl = nullptr;
-            int nt = 0, mr = 0;
-            if (build_direct(ids, dt, &tl, &nt, &mr) < 0) return false;
-            const float ms = time_ms([&] { return launch_direct_worlds(dt[0], tl, nt, mr, b.stream); });
-            out = double(ms) / t;
-            return true;
-        };
-        double cost_all = 0.0, cost_tap[3] = {0.0, 0.0, 0.0};
-        if (!dall.empty() && !time_direct(dall, taps_all, cost_all)) return LENIA_ERR_CUDA;
-        for (int bd = 0; bd < 3; ++bd) {
-            cost_tap[bd] = cost_all;
-            if (taps[bd] >= 1e8 && !time_direct(dcand[bd], taps[bd], cost_tap[bd])) return LENIA_ERR_CUDA;
+
+        // Spectral classes for every world that might take the spectral path.
+        std::map<std::pair<int, int>, int> class_of;
+        std::vector<int> cls(n, -1);
+        for (uint32_t i = 0; i < n; ++i)
+            if (can_fft[i]) {
+                auto key = std::make_pair(int(worlds[i].width), int(worlds[i].height));
+                auto it = class_of.find(key);
+                if (it == class_of.end()) {
+                    BatchContext::SizeClass c;
+                    c.W = key.first;
+                    c.H = key.second;
+                    c.M = c.W / 2;
+                    class_of[key] = int(b.classes.size());
+                    b.classes.push_back(c);
+                    it = class_of.find(key);
+                }
+                cls[i] = it->second;
+            }
+
+        // Per-world parameters and the substep seed base.
+        std::vector<StepParams> params(n);
+        std::vector<uint32_t> base_seed(n);
+        for (uint32_t i = 0; i < n; ++i) {
+            params[i] = world_params(worlds[i]);
+            base_seed[i] = derive_seed(worlds[i].seed, 0x4C454E31u);
         }
-        std::vector<double> cost_px(b.classes.size(), 0.0);
+        std::vector<std::vector<int>> class_members(b.classes.size());
+        for (uint32_t i = 0; i < n; ++i)
+            if (cls[i] >= 0) class_members[size_t(cls[i])].push_back(int(i));
+
+        // Spectral resources of every candidate world of each size class.
         for (size_t ci = 0; ci < b.classes.size(); ++ci) {
             auto& c = b.classes[ci];
-            SpectralWorld* st[2] = {nullptr, nullptr};
-            SpectralWorld* rt[2] = {nullptr, nullptr};
-            if (build_spectral(ci, class_members[ci], st, rt) < 0) return LENIA_ERR_CUDA;
             const int cnt = int(class_members[ci].size());
-            const float ms = time_ms([&] {
-                cudaError_t r = launch_col_fast_worlds(c.H, c.M, c.t, c.col_batch, st[0], cnt, b.stream);
-                if (r == cudaSuccess) r = launch_row_fast_worlds(c.H, c.M, c.t, c.tw_r2c, c.row_batch, st[0], cnt, b.stream);
-                return r;
-            });
-            cost_px[ci] = double(ms) / (double(c.W) * c.H * cnt);
-        }
-        cudaEventDestroy(ea);
-        cudaEventDestroy(eb);
-        for (uint32_t i = 0; i < n; ++i)
-            if (can_direct[i] && can_fft[i])
-                b.path[i] = (cost_tap[band(i)] * nnz[i] <= cost_px[size_t(cls[i])]) ? LENIA_CONV_DIRECT : LENIA_CONV_FFT;
-        cudaMemsetAsync(b.fields, 0, total * sizeof(float), b.stream);
-    }
-
-    // Final tables.
-    for (uint32_t i = 0; i < n; ++i)
-        if (b.path[i] == LENIA_CONV_DIRECT) b.direct_ids.push_back(int(i));
-    if (build_direct(b.direct_ids, b.d_dtab, &b.d_tiles, &b.ntiles, &b.max_r) < 0) return LENIA_ERR_CUDA;
-    std::vector<BatchContext::SizeClass> kept;
-    for (size_t ci = 0; ci < b.classes.size(); ++ci) {
-        auto& c = b.classes[ci];
-        for (int wi : class_members[ci])
-            if (b.path[size_t(wi)] == LENIA_CONV_FFT) c.ids.push_back(wi);
-        if (c.ids.empty()) continue;
-        if (build_spectral(ci, c.ids, c.d_stab, c.d_r2c) < 0) return LENIA_ERR_CUDA;
-        kept.push_back(c);
-    }
-    b.classes = kept;
-
-    // Columns / rows per CTA iteration of each size's passes: every candidate
-    // timed on the class's own tables (the fields are cleared afterwards).
-    if (!b.classes.empty()) {
-        cudaEvent_t ea, eb;
-        cudaEventCreate(&ea);
-        cudaEventCreate(&eb);
-        auto time_ms = [&](auto&& fn) {
-            float best = 1e30f;
-            for (int rep = 0; rep < 3; ++rep) {
-                cudaEventRecord(ea, b.stream);
-                if (fn() != cudaSuccess) return 1e30f;
-                cudaEventRecord(eb, b.stream);
-                cudaEventSynchronize(eb);
-                float ms = 0.0f;
-                cudaEventElapsedTime(&ms, ea, eb);
-                if (rep > 0) best = std::min(best, ms);
+            const size_t spec = size_t(c.M) * c.H;
+            const int Hh = c.H / 2 + 1;
+            if ((e = b.alloc(&c.S, spec * cnt)) != cudaSuccess) return LENIA_ERR_CUDA;
+            if ((e = b.alloc(&c.U, spec * cnt)) != cudaSuccess) return LENIA_ERR_CUDA;
+            if ((e = b.alloc(&c.khat, size_t(c.M + 1) * Hh * cnt)) != cudaSuccess) return LENIA_ERR_CUDA;
+            std::vector<float> kh(size_t(c.M + 1) * Hh * cnt), img, sp;
+            for (int k = 0; k < cnt; ++k) {
+                const lenia_world& w = worlds[class_members[ci][size_t(k)]];
+                build_ring_image(w.width, w.height, float(w.radius), w.shell_sigma, std::vector<float>{1.0f},
+                                 w.kernel_core, img);
+                kernel_spectrum(img, w.width, w.height, sp);
+                std::copy(sp.begin(), sp.end(), kh.begin() + size_t(k) * (c.M + 1) * Hh);
             }
-            return best;
+            cudaMemcpy(c.khat, kh.data(), kh.size() * sizeof(float), cudaMemcpyHostToDevice);
+            std::vector<float2> t2;
+            fill_twiddles(c.W, t2);
+            t2.resize(size_t(c.M) + 1);
+            if ((e = b.alloc(&c.tw_r2c, t2.size())) != cudaSuccess) return LENIA_ERR_CUDA;
+            cudaMemcpy(c.tw_r2c, t2.data(), t2.size() * sizeof(float2), cudaMemcpyHostToDevice);
+            FastPlan cf, ri;
+            fast_col_plan(c.H, cf);
+            fast_row_plan(c.M, ri);
+            FastPlan rcf = cf, rri = ri;
+            for (int i = 0; i < cf.np; ++i) rcf.radix[i] = cf.radix[cf.np - 1 - i];
+            for (int i = 0; i < ri.np; ++i) rri.radix[i] = ri.radix[ri.np - 1 - i];
+            const FastPlan* plans[4] = {&cf, &rcf, &ri, &rri};
+            for (int q = 0; q < 4; ++q) {
+                std::vector<float2> tw;
+                fast_plan_twiddles(*plans[q], tw);
+                if (tw.empty()) tw.push_back(make_float2(1.0f, 0.0f));
+                if ((e = b.alloc(&c.tw[q], tw.size())) != cudaSuccess) return LENIA_ERR_CUDA;
+                cudaMemcpy(c.tw[q], tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice);
+            }
+            c.t.col_twf = c.tw[0];
+            c.t.col_twi = c.tw[1];
+            c.t.row_twi = c.tw[2];
+            c.t.row_twf = c.tw[3];
+        }
+
+        std::vector<int> slot_of(n, 0);
+        // Direct tables for a set of worlds (both parities) and their tile list.
+        auto build_direct = [&](const std::vector<int>& ids, DirectWorld** dtab, int3** dtiles, int* ntiles,
+                                int* max_r) -> int {
+            std::vector<float> all_w;
+            std::vector<uint32_t> all_s;
+            std::vector<DirectWorld> tab;
+            std::vector<int3> tiles;
+            std::vector<std::pair<size_t, size_t>> offs;
+            *max_r = 0;
+            for (int i : ids) {
+                const int R = int(worlds[i].radius);
+                DirectGeometry g{R, 2 * R + 1, (R + 3) / 4 * 4, 0};
+                g.wp = 2 * g.xp + 8;
+                const size_t wo = all_w.size(), so = all_s.size();
+                all_w.resize(wo + size_t(g.ksize) * g.wp, 0.0f);
+                all_s.resize(so + size_t(g.ksize), 128u);
+                for (int dy = 0; dy < g.ksize; ++dy) {
+                    int lo = 1 << 30, hi = -(1 << 30);
+                    for (int dx = -R; dx <= R; ++dx) {
+                        const float v = luts[size_t(i)][size_t(dy) * g.ksize + size_t(dx + R)];
+                        all_w[wo + size_t(dy) * g.wp + size_t(dx + g.xp)] = v;
+                        if (v != 0.0f) { lo = std::min(lo, dx); hi = std::max(hi, dx); }
+                    }
+                    if (lo <= hi) {
+                        const int start = (lo >= 0) ? (lo / 4) * 4 : -((-lo + 3) / 4) * 4;
+                        all_s[so + size_t(dy)] = uint32_t(start + 128) | (uint32_t((hi - start + 1 + 7) / 8) << 16);
+                    }
+                }
+                offs.push_back({wo, so});
+                DirectWorld dw{};
+                dw.g = g;
+                dw.p = params[size_t(i)];
+                slot_of[size_t(i)] = int(tab.size());
+                for (int ty = 0; ty < (int(worlds[i].height) + 15) / 16; ++ty)
+                    for (int tx = 0; tx < (int(worlds[i].width) + 31) / 32; ++tx)
+                        tiles.push_back(make_int3(int(tab.size()), tx, ty));
+                tab.push_back(dw);
+                *max_r = std::max(*max_r, R);
+            }
+            *ntiles = int(tiles.size());
+            if (tab.empty()) return LENIA_OK;
+            float* dw = nullptr;
+            uint32_t* ds = nullptr;
+            if (b.alloc(&dw, all_w.size()) != cudaSuccess || b.alloc(&ds, all_s.size()) != cudaSuccess ||
+                b.alloc(dtiles, tiles.size()) != cudaSuccess || b.alloc(&dtab[0], tab.size()) != cudaSuccess ||
+                b.alloc(&dtab[1], tab.size()) != cudaSuccess)
+                return LENIA_ERR_CUDA;
+            cudaMemcpy(dw, all_w.data(), all_w.size() * sizeof(float), cudaMemcpyHostToDevice);
+            cudaMemcpy(ds, all_s.data(), all_s.size() * sizeof(uint32_t), cudaMemcpyHostToDevice);
+            cudaMemcpy(*dtiles, tiles.data(), tiles.size() * sizeof(int3), cudaMemcpyHostToDevice);
+            for (int par = 0; par < 2; ++par) {
+                std::vector<DirectWorld> t2 = tab;
+                for (size_t k = 0; k < t2.size(); ++k) {
+                    t2[k].weights = dw + offs[k].first;
+                    t2[k].spans = ds + offs[k].second;
+                    t2[k].src = b.field(ids[k], par);
+                    t2[k].dst = b.field(ids[k], par ^ 1);
+                }
+                cudaMemcpy(dtab[par], t2.data(), t2.size() * sizeof(DirectWorld), cudaMemcpyHostToDevice);
+            }
+            return LENIA_OK;
         };
-        for (auto& c : b.classes) {
-            const int cnt = int(c.ids.size());
-            float best = 1e30f;
-            for (int cb : {8, 4, 2}) {
-                const float ms = time_ms([&] { return launch_col_fast_worlds(c.H, c.M, c.t, cb, c.d_stab[0], cnt, b.stream); });
-                if (ms < 0.97f * best) { best = ms; c.col_batch = cb; }
+        // Spectral tables of one class for a subset of its candidate worlds.
+        auto build_spectral = [&](size_t ci, const std::vector<int>& ids, SpectralWorld** stab, SpectralWorld** r2c) -> int {
+            auto& c = b.classes[ci];
+            const size_t spec = size_t(c.M) * c.H;
+            const int Hh = c.H / 2 + 1;
+            std::vector<SpectralWorld> steady[2], rt[2];
+            for (int wi : ids) {
+                const size_t k = size_t(std::find(class_members[ci].begin(), class_members[ci].end(), wi) -
+                                        class_members[ci].begin());
+                slot_of[size_t(wi)] = int(steady[0].size());
+                for (int par = 0; par < 2; ++par) {
+                    SpectralWorld sw{};
+                    sw.S = c.S + spec * k;
+                    sw.U = c.U + spec * k;
+                    sw.khat = c.khat + size_t(c.M + 1) * Hh * k;
+                    sw.A = b.field(wi, par);
+                    sw.A_out = b.field(wi, par ^ 1);
+                    sw.S_next = c.S + spec * k;
+                    sw.M = c.M;
+                    sw.nk = 1;
+                    sw.p = params[size_t(wi)];
+                    steady[par].push_back(sw);
+                    SpectralWorld r = sw;
+                    r.nk = 0;  // row spectrum of A only
+                    r.A_out = nullptr;
+                    r.U = nullptr;
+                    rt[par].push_back(r);
+                }
             }
-            best = 1e30f;
-            for (int rb : kRowCandidates) {
+            if (ids.empty()) return LENIA_OK;
+            for (int par = 0; par < 2; ++par) {
+                if (b.alloc(&stab[par], steady[par].size()) != cudaSuccess || b.alloc(&r2c[par], rt[par].size()) != cudaSuccess)
+                    return LENIA_ERR_CUDA;
+                cudaMemcpy(stab[par], steady[par].data(), steady[par].size() * sizeof(SpectralWorld), cudaMemcpyHostToDevice);
+                cudaMemcpy(r2c[par], rt[par].data(), rt[par].size() * sizeof(SpectralWorld), cudaMemcpyHostToDevice);
+            }
+            return LENIA_OK;
+        };
+
+        // Autotuner (policy AUTO): time the batched direct launch over every
+        // direct candidate (cost per pixel-tap) and each class's spectral step
+        // over all its candidates (cost per pixel) -- the batch's own launch
+        // shapes, on its own buffers -- and give each world the cheaper path.
+        if (policy == LENIA_BATCH_AUTO) {
+            cudaEvent_t ea, eb;
+            cudaEventCreate(&ea);
+            cudaEventCreate(&eb);
+            auto time_ms = [&](auto&& fn) {
+                float best = 1e30f;
+                for (int rep = 0; rep < 3; ++rep) {
+                    cudaEventRecord(ea, b.stream);
+                    if (fn() != cudaSuccess) return 1e30f;
+                    cudaEventRecord(eb, b.stream);
+                    cudaEventSynchronize(eb);
+                    float ms = 0.0f;
+                    cudaEventElapsedTime(&ms, ea, eb);
+                    if (rep > 0) best = std::min(best, ms);
+                }
+                return best;
+            };
+            // Cost per tap of the batched direct launch over every candidate.
+            // That launch sizes its halo tile for the largest radius it holds,
+            // which overstates the cost for small radii; so candidates are also
+            // timed in radius bands, each with its own halo, and a band with
+            // enough work (>= 1e8 pixel-taps, so the launch itself is amortised)
+            // uses its own figure.
+            const auto band = [&](uint32_t i) { return worlds[i].radius <= 12u ? 0 : worlds[i].radius <= 20u ? 1 : 2; };
+            std::vector<int> dall, dcand[3];
+            double taps_all = 0.0, taps[3] = {0.0, 0.0, 0.0};
+            for (uint32_t i = 0; i < n; ++i)
+                if (can_direct[i] && can_fft[i]) {
+                    const double t = double(worlds[i].width) * worlds[i].height * nnz[i];
+                    dall.push_back(int(i));
+                    dcand[band(i)].push_back(int(i));
+                    taps_all += t;
+                    taps[band(i)] += t;
+                }
+            const auto time_direct = [&](const std::vector<int>& ids, double t, double& out) {
+                DirectWorld* dt[2] = {nullptr, nullptr};
+                int3* tl = nullptr;
+                int nt = 0, mr = 0;
+                if (build_direct(ids, dt, &tl, &nt, &mr) < 0) return false;
+                const float ms = time_ms([&] { return launch_direct_worlds(dt[0], tl, nt, mr, b.stream); });
+                out = double(ms) / t;
+                return true;
+            };
+            double cost_all = 0.0, cost_tap[3] = {0.0, 0.0, 0.0};
+            if (!dall.empty() && !time_direct(dall, taps_all, cost_all)) return LENIA_ERR_CUDA;
+            for (int bd = 0; bd < 3; ++bd) {
+                cost_tap[bd] = cost_all;
+                if (taps[bd] >= 1e8 && !time_direct(dcand[bd], taps[bd], cost_tap[bd])) return LENIA_ERR_CUDA;
+            }
+            std::vector<double> cost_px(b.classes.size(), 0.0);
+            for (size_t ci = 0; ci < b.classes.size(); ++ci) {
+                auto& c = b.classes[ci];
+                SpectralWorld* st[2] = {nullptr, nullptr};
+                SpectralWorld* rt[2] = {nullptr, nullptr};
+                if (build_spectral(ci, class_members[ci], st, rt) < 0) return LENIA_ERR_CUDA;
+                const int cnt = int(class_members[ci].size());
                 const float ms = time_ms([&] {
-                    return launch_row_fast_worlds(c.H, c.M, c.t, c.tw_r2c, rb, c.d_stab[0], cnt, b.stream);
+                    cudaError_t r = launch_col_fast_worlds(c.H, c.M, c.t, c.col_batch, st[0], cnt, b.stream);
+                    if (r == cudaSuccess) r = launch_row_fast_worlds(c.H, c.M, c.t, c.tw_r2c, c.row_batch, st[0], cnt, b.stream);
+                    return r;
                 });
-                if (ms < 0.97f * best) { best = ms; c.row_batch = rb; }
+                cost_px[ci] = double(ms) / (double(c.W) * c.H * cnt);
             }
+            cudaEventDestroy(ea);
+            cudaEventDestroy(eb);
+            for (uint32_t i = 0; i < n; ++i)
+                if (can_direct[i] && can_fft[i])
+                    b.path[i] = (cost_tap[band(i)] * nnz[i] <= cost_px[size_t(cls[i])]) ? LENIA_CONV_DIRECT : LENIA_CONV_FFT;
+            cudaMemsetAsync(b.fields, 0, total * sizeof(float), b.stream);
         }
-        cudaGetLastError();
-        cudaEventDestroy(ea);
-        cudaEventDestroy(eb);
-        cudaMemsetAsync(b.fields, 0, total * sizeof(float), b.stream);
-    }
 
-    // Per-world seed/frame state and where each world's parameters live in
-    // the two parity tables (device addresses, for the advance kernel).
-    std::vector<StepParams*> loc(2 * size_t(n), nullptr);
-    for (uint32_t i = 0; i < n; ++i)
-        for (int par = 0; par < 2; ++par) {
-            char* entry = nullptr;
-            size_t member = 0;
-            if (b.path[i] == LENIA_CONV_DIRECT) {
-                entry = reinterpret_cast<char*>(b.d_dtab[par] + slot_of[i]);
-                member = offsetof(DirectWorld, p);
-            } else {
-                for (auto& c : b.classes)
-                    if (c.W == int(worlds[i].width) && c.H == int(worlds[i].height))
-                        entry = reinterpret_cast<char*>(c.d_stab[par] + slot_of[i]);
-                member = offsetof(SpectralWorld, p);
+        // Final tables.
+        for (uint32_t i = 0; i < n; ++i)
+            if (b.path[i] == LENIA_CONV_DIRECT) b.direct_ids.push_back(int(i));
+        if (build_direct(b.direct_ids, b.d_dtab, &b.d_tiles, &b.ntiles, &b.max_r) < 0) return LENIA_ERR_CUDA;
+        std::vector<BatchContext::SizeClass> kept;
+        for (size_t ci = 0; ci < b.classes.size(); ++ci) {
+            auto& c = b.classes[ci];
+            for (int wi : class_members[ci])
+                if (b.path[size_t(wi)] == LENIA_CONV_FFT) c.ids.push_back(wi);
+            if (c.ids.empty()) continue;
+            if (build_spectral(ci, c.ids, c.d_stab, c.d_r2c) < 0) return LENIA_ERR_CUDA;
+            kept.push_back(c);
+        }
+        b.classes = kept;
+
+        // Columns / rows per CTA iteration of each size's passes: every candidate
+        // timed on the class's own tables (the fields are cleared afterwards).
+        if (!b.classes.empty()) {
+            cudaEvent_t ea, eb;
+            cudaEventCreate(&ea);
+            cudaEventCreate(&eb);
+            auto time_ms = [&](auto&& fn) {
+                float best = 1e30f;
+                for (int rep = 0; rep < 3; ++rep) {
+                    cudaEventRecord(ea, b.stream);
+                    if (fn() != cudaSuccess) return 1e30f;
+                    cudaEventRecord(eb, b.stream);
+                    cudaEventSynchronize(eb);
+                    float ms = 0.0f;
+                    cudaEventElapsedTime(&ms, ea, eb);
+                    if (rep > 0) best = std::min(best, ms);
+                }
+                return best;
+            };
+            for (auto& c : b.classes) {
+                const int cnt = int(c.ids.size());
+                float best = 1e30f;
+                for (int cb : {8, 4, 2}) {
+                    const float ms = time_ms([&] { return launch_col_fast_worlds(c.H, c.M, c.t, cb, c.d_stab[0], cnt, b.stream); });
+                    if (ms < 0.97f * best) { best = ms; c.col_batch = cb; }
+                }
+                best = 1e30f;
+                for (int rb : kRowCandidates) {
+                    const float ms = time_ms([&] {
+                        return launch_row_fast_worlds(c.H, c.M, c.t, c.tw_r2c, rb, c.d_stab[0], cnt, b.stream);
+                    });
+                    if (ms < 0.97f * best) { best = ms; c.row_batch = rb; }
+                }
             }
-            loc[2 * i + size_t(par)] = reinterpret_cast<StepParams*>(entry + member);
+            cudaGetLastError();
+            cudaEventDestroy(ea);
+            cudaEventDestroy(eb);
+            cudaMemsetAsync(b.fields, 0, total * sizeof(float), b.stream);
         }
-    if (b.alloc(&b.d_param_loc, loc.size()) != cudaSuccess || b.alloc(&b.d_base_seed, n) != cudaSuccess ||
-        b.alloc(&b.d_frame, n) != cudaSuccess)
-        return LENIA_ERR_CUDA;
-    cudaMemcpy(b.d_param_loc, loc.data(), loc.size() * sizeof(StepParams*), cudaMemcpyHostToDevice);
-    cudaMemcpy(b.d_base_seed, base_seed.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice);
-    cudaMemset(b.d_frame, 0, n * sizeof(uint32_t));
+
+        // Per-world seed/frame state and where each world's parameters live in
+        // the two parity tables (device addresses, for the advance kernel).
+        std::vector<StepParams*> loc(2 * size_t(n), nullptr);
+        for (uint32_t i = 0; i < n; ++i)
+            for (int par = 0; par < 2; ++par) {
+                char* entry = nullptr;
+                size_t member = 0;
+                if (b.path[i] == LENIA_CONV_DIRECT) {
+                    entry = reinterpret_cast<char*>(b.d_dtab[par] + slot_of[i]);
+                    member = offsetof(DirectWorld, p);
+                } else {
+                    for (auto& c : b.classes)
+                        if (c.W == int(worlds[i].width) && c.H == int(worlds[i].height))
+                            entry = reinterpret_cast<char*>(c.d_stab[par] + slot_of[i]);
+                    member = offsetof(SpectralWorld, p);
+                }
+                loc[2 * i + size_t(par)] = reinterpret_cast<StepParams*>(entry + member);
+            }
+        if (b.alloc(&b.d_param_loc, loc.size()) != cudaSuccess || b.alloc(&b.d_base_seed, n) != cudaSuccess ||
+            b.alloc(&b.d_frame, n) != cudaSuccess)
+            return LENIA_ERR_CUDA;
+        cudaMemcpy(b.d_param_loc, loc.data(), loc.size() * sizeof(StepParams*), cudaMemcpyHostToDevice);
+        cudaMemcpy(b.d_base_seed, base_seed.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice);
+        cudaMemset(b.d_frame, 0, n * sizeof(uint32_t));
 
 
-    // Stats tables.
-    std::vector<const float*> fp0(n), fp1(n);
-    std::vector<int> npx(n);
-    for (uint32_t i = 0; i < n; ++i) {
-        fp0[i] = b.field(int(i), 0);
-        fp1[i] = b.field(int(i), 1);
-        npx[i] = int(worlds[i].width * worlds[i].height);
-    }
-    if (b.alloc(&b.d_field_ptrs[0], n) != cudaSuccess || b.alloc(&b.d_field_ptrs[1], n) != cudaSuccess ||
-        b.alloc(&b.d_npx, n) != cudaSuccess || b.alloc(&b.d_stats, 2 * size_t(n)) != cudaSuccess)
-        return LENIA_ERR_CUDA;
-    cudaMemcpy(b.d_field_ptrs[0], fp0.data(), n * sizeof(float*), cudaMemcpyHostToDevice);
-    cudaMemcpy(b.d_field_ptrs[1], fp1.data(), n * sizeof(float*), cudaMemcpyHostToDevice);
-    cudaMemcpy(b.d_npx, npx.data(), n * sizeof(int), cudaMemcpyHostToDevice);
+        // Stats tables.
+        std::vector<const float*> fp0(n), fp1(n);
+        std::vector<int> npx(n);
+        for (uint32_t i = 0; i < n; ++i) {
+            fp0[i] = b.field(int(i), 0);
+            fp1[i] = b.field(int(i), 1);
+            npx[i] = int(worlds[i].width * worlds[i].height);
+        }
+        if (b.alloc(&b.d_field_ptrs[0], n) != cudaSuccess || b.alloc(&b.d_field_ptrs[1], n) != cudaSuccess ||
+            b.alloc(&b.d_npx, n) != cudaSuccess || b.alloc(&b.d_stats, 2 * size_t(n)) != cudaSuccess)
+            return LENIA_ERR_CUDA;
+        cudaMemcpy(b.d_field_ptrs[0], fp0.data(), n * sizeof(float*), cudaMemcpyHostToDevice);
+        cudaMemcpy(b.d_field_ptrs[1], fp1.data(), n * sizeof(float*), cudaMemcpyHostToDevice);
+        cudaMemcpy(b.d_npx, npx.data(), n * sizeof(int), cudaMemcpyHostToDevice);
 
-    cudaStreamSynchronize(b.stream);
-    if ((e = cudaGetLastError()) != cudaSuccess) {
-        b.message = std::string("batch setup: ") + cudaGetErrorString(e);
-        return LENIA_ERR_CUDA;
-    }
-    *out = holder.release();
-    return LENIA_OK;
+        cudaStreamSynchronize(b.stream);
+        if ((e = cudaGetLastError()) != cudaSuccess) {
+            b.message = std::string("batch setup: ") + cudaGetErrorString(e);
+            return LENIA_ERR_CUDA;
+        }
+        *out = holder.release();
+        return LENIA_OK;
+    });
+    // A failure the body reported on the batch it was building.
+    if (rc < 0 && holder && g_batch_create_error.empty()) g_batch_create_error = holder->ctx.message;
+    return rc;
 }
 
 int lenia_batch_destroy(lenia_batch* b) {
-    if (!b) return LENIA_ERR_INVALID_ARG;
-    delete b;
-    return LENIA_OK;
+    return lenia::abi_guard(b ? &b->ctx.message : nullptr, [&]() -> int {
+        if (!b) return LENIA_ERR_INVALID_ARG;
+        delete b;
+        return LENIA_OK;
+    });
 }
 
 int lenia_batch_upload(lenia_batch* bb, uint32_t world, const float* host) {
-    if (!bb || !host || world >= bb->ctx.worlds.size()) return LENIA_ERR_INVALID_ARG;
-    BatchContext& b = bb->ctx;
-    const lenia_world& w = b.worlds[world];
-    cudaError_t e = cudaMemcpyAsync(b.field(int(world), b.cur), host, sizeof(float) * w.width * w.height,
-                                    cudaMemcpyHostToDevice, b.stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(b.stream);
-    b.spectra_valid = false;
-    return e == cudaSuccess ? LENIA_OK : b.fail(LENIA_ERR_CUDA, cudaGetErrorString(e));
+    return lenia::abi_guard(bb ? &bb->ctx.message : nullptr, [&]() -> int {
+        if (!bb || !host || world >= bb->ctx.worlds.size()) return LENIA_ERR_INVALID_ARG;
+        BatchContext& b = bb->ctx;
+        const lenia_world& w = b.worlds[world];
+        cudaError_t e = cudaMemcpyAsync(b.field(int(world), b.cur), host, sizeof(float) * w.width * w.height,
+                                        cudaMemcpyHostToDevice, b.stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(b.stream);
+        b.spectra_valid = false;
+        return e == cudaSuccess ? LENIA_OK : b.fail(LENIA_ERR_CUDA, cudaGetErrorString(e));
+    });
 }
 
 int lenia_batch_download(lenia_batch* bb, uint32_t world, float* host) {
-    if (!bb || !host || world >= bb->ctx.worlds.size()) return LENIA_ERR_INVALID_ARG;
-    BatchContext& b = bb->ctx;
-    const lenia_world& w = b.worlds[world];
-    cudaError_t e = cudaDeviceSynchronize();
-    if (e == cudaSuccess)
-        e = cudaMemcpyAsync(host, b.field(int(world), b.cur), sizeof(float) * w.width * w.height,
-                            cudaMemcpyDeviceToHost, b.stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(b.stream);
-    return e == cudaSuccess ? LENIA_OK : b.fail(LENIA_ERR_CUDA, cudaGetErrorString(e));
+    return lenia::abi_guard(bb ? &bb->ctx.message : nullptr, [&]() -> int {
+        if (!bb || !host || world >= bb->ctx.worlds.size()) return LENIA_ERR_INVALID_ARG;
+        BatchContext& b = bb->ctx;
+        const lenia_world& w = b.worlds[world];
+        cudaError_t e = cudaDeviceSynchronize();
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(host, b.field(int(world), b.cur), sizeof(float) * w.width * w.height,
+                                cudaMemcpyDeviceToHost, b.stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(b.stream);
+        return e == cudaSuccess ? LENIA_OK : b.fail(LENIA_ERR_CUDA, cudaGetErrorString(e));
+    });
 }
 
 int lenia_batch_step(lenia_batch* bb, uint32_t steps, void* stream) {
-    using namespace lenia;
-    if (!bb) return LENIA_ERR_INVALID_ARG;
-    BatchContext& b = bb->ctx;
-    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : b.stream;
-    const int n = int(b.worlds.size());
-    cudaError_t e = cudaSuccess;
-    if (!b.spectra_valid) {
-        e = b.launch_r2c(b.cur, s);
-        if (e != cudaSuccess) return b.fail(LENIA_ERR_CUDA, std::string("row spectra: ") + cudaGetErrorString(e));
-        b.spectra_valid = true;
-    }
-    if (steps == 0) return LENIA_OK;
-    // The graph for (steps, parity): substeps alternate the parity of the
-    // tables; after each, the device advances seeds and frames.
-    const auto key = std::make_pair(steps, b.cur);
-    auto it = b.graphs.find(key);
-    if (it == b.graphs.end()) {
-        cudaStream_t cap = b.stream;
-        cudaGraph_t graph = nullptr;
-        e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
-        if (e != cudaSuccess) return b.fail(LENIA_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e));
-        int par = b.cur;
-        for (uint32_t k = 0; k < steps && e == cudaSuccess; ++k) {
-            e = b.launch_step(par, cap);
-            if (e == cudaSuccess) {
-                advance_kernel<<<(n + 127) / 128, 128, 0, cap>>>(b.d_param_loc, n, b.d_base_seed, b.d_frame);
-                e = cudaGetLastError();
-            }
-            par ^= 1;
+    return lenia::abi_guard(bb ? &bb->ctx.message : nullptr, [&]() -> int {
+        using namespace lenia;
+        if (!bb) return LENIA_ERR_INVALID_ARG;
+        BatchContext& b = bb->ctx;
+        cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : b.stream;
+        const int n = int(b.worlds.size());
+        cudaError_t e = cudaSuccess;
+        if (!b.spectra_valid) {
+            e = b.launch_r2c(b.cur, s);
+            if (e != cudaSuccess) return b.fail(LENIA_ERR_CUDA, std::string("row spectra: ") + cudaGetErrorString(e));
+            b.spectra_valid = true;
         }
-        cudaError_t e2 = cudaStreamEndCapture(cap, &graph);
-        if (e == cudaSuccess) e = e2;
-        cudaGraphExec_t exec = nullptr;
-        if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
-        if (graph) cudaGraphDestroy(graph);
-        if (e != cudaSuccess) return b.fail(LENIA_ERR_CUDA, std::string("graph: ") + cudaGetErrorString(e));
-        it = b.graphs.emplace(key, exec).first;
-    }
-    e = cudaGraphLaunch(it->second, s);
-    if (e != cudaSuccess) return b.fail(LENIA_ERR_CUDA, std::string("graph launch: ") + cudaGetErrorString(e));
-    if (steps % 2) b.cur ^= 1;
-    return LENIA_OK;
+        if (steps == 0) return LENIA_OK;
+        // The graph for (steps, parity): substeps alternate the parity of the
+        // tables; after each, the device advances seeds and frames.
+        const auto key = std::make_pair(steps, b.cur);
+        auto it = b.graphs.find(key);
+        if (it == b.graphs.end()) {
+            cudaStream_t cap = b.stream;
+            cudaGraph_t graph = nullptr;
+            e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+            if (e != cudaSuccess) return b.fail(LENIA_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e));
+            int par = b.cur;
+            for (uint32_t k = 0; k < steps && e == cudaSuccess; ++k) {
+                e = b.launch_step(par, cap);
+                if (e == cudaSuccess) {
+                    advance_kernel<<<(n + 127) / 128, 128, 0, cap>>>(b.d_param_loc, n, b.d_base_seed, b.d_frame);
+                    e = cudaGetLastError();
+                }
+                par ^= 1;
+            }
+            cudaError_t e2 = cudaStreamEndCapture(cap, &graph);
+            if (e == cudaSuccess) e = e2;
+            cudaGraphExec_t exec = nullptr;
+            if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+            if (graph) cudaGraphDestroy(graph);
+            if (e != cudaSuccess) return b.fail(LENIA_ERR_CUDA, std::string("graph: ") + cudaGetErrorString(e));
+            it = b.graphs.emplace(key, exec).first;
+        }
+        e = cudaGraphLaunch(it->second, s);
+        if (e != cudaSuccess) return b.fail(LENIA_ERR_CUDA, std::string("graph launch: ") + cudaGetErrorString(e));
+        if (steps % 2) b.cur ^= 1;
+        return LENIA_OK;
+    });
 }
 
 int lenia_batch_stats(lenia_batch* bb, double* mean, double* var) {
-    if (!bb || !mean || !var) return LENIA_ERR_INVALID_ARG;
-    BatchContext& b = bb->ctx;
-    const int n = int(b.worlds.size());
-    cudaError_t e = cudaMemsetAsync(b.d_stats, 0, sizeof(double) * 2 * n, b.stream);
-    if (e == cudaSuccess) {
-        lenia::stats_kernel<<<dim3(16, unsigned(n)), 256, 0, b.stream>>>(b.d_field_ptrs[b.cur], b.d_npx, b.d_stats, n);
-        e = cudaGetLastError();
-    }
-    std::vector<double> h(2 * size_t(n));
-    if (e == cudaSuccess) e = cudaDeviceSynchronize();
-    if (e == cudaSuccess) e = cudaMemcpy(h.data(), b.d_stats, h.size() * sizeof(double), cudaMemcpyDeviceToHost);
-    if (e != cudaSuccess) return b.fail(LENIA_ERR_CUDA, cudaGetErrorString(e));
-    for (int i = 0; i < n; ++i) {
-        const double cnt = double(b.worlds[size_t(i)].width) * b.worlds[size_t(i)].height;
-        mean[i] = h[2 * size_t(i)] / cnt;
-        var[i] = std::max(0.0, h[2 * size_t(i) + 1] / cnt - mean[i] * mean[i]);
-    }
-    return LENIA_OK;
+    return lenia::abi_guard(bb ? &bb->ctx.message : nullptr, [&]() -> int {
+        if (!bb || !mean || !var) return LENIA_ERR_INVALID_ARG;
+        BatchContext& b = bb->ctx;
+        const int n = int(b.worlds.size());
+        cudaError_t e = cudaMemsetAsync(b.d_stats, 0, sizeof(double) * 2 * n, b.stream);
+        if (e == cudaSuccess) {
+            lenia::stats_kernel<<<dim3(16, unsigned(n)), 256, 0, b.stream>>>(b.d_field_ptrs[b.cur], b.d_npx, b.d_stats, n);
+            e = cudaGetLastError();
+        }
+        std::vector<double> h(2 * size_t(n));
+        if (e == cudaSuccess) e = cudaDeviceSynchronize();
+        if (e == cudaSuccess) e = cudaMemcpy(h.data(), b.d_stats, h.size() * sizeof(double), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return b.fail(LENIA_ERR_CUDA, cudaGetErrorString(e));
+        for (int i = 0; i < n; ++i) {
+            const double cnt = double(b.worlds[size_t(i)].width) * b.worlds[size_t(i)].height;
+            mean[i] = h[2 * size_t(i)] / cnt;
+            var[i] = std::max(0.0, h[2 * size_t(i) + 1] / cnt - mean[i] * mean[i]);
+        }
+        return LENIA_OK;
+    });
 }
 
 int lenia_batch_activity(lenia_batch* bb, const lenia_colormap* cm, double* mean_luma, double* stddev_luma) {
-    if (!bb || !cm || !mean_luma || !stddev_luma) return LENIA_ERR_INVALID_ARG;
-    BatchContext& b = bb->ctx;
-    const int n = int(b.worlds.size());
-    static_assert(sizeof(lenia_colormap) == sizeof(lenia::ColorMapParams), "colour map layout");
-    lenia::ColorMapParams p;
-    std::memcpy(&p, cm, sizeof(p));
-    cudaError_t e = cudaMemsetAsync(b.d_stats, 0, sizeof(double) * 2 * n, b.stream);
-    if (e == cudaSuccess) {
-        lenia::activity_kernel<<<dim3(16, unsigned(n)), 256, 0, b.stream>>>(b.d_field_ptrs[b.cur], b.d_npx, p,
-                                                                            b.d_stats, n);
-        e = cudaGetLastError();
-    }
-    std::vector<double> h(2 * size_t(n));
-    if (e == cudaSuccess) e = cudaDeviceSynchronize();
-    if (e == cudaSuccess) e = cudaMemcpy(h.data(), b.d_stats, h.size() * sizeof(double), cudaMemcpyDeviceToHost);
-    if (e != cudaSuccess) return b.fail(LENIA_ERR_CUDA, cudaGetErrorString(e));
-    for (int i = 0; i < n; ++i) {
-        const double cnt = double(b.worlds[size_t(i)].width) * b.worlds[size_t(i)].height;
-        const double mean = h[2 * size_t(i)] / cnt;
-        mean_luma[i] = mean;
-        stddev_luma[i] = std::sqrt(std::max(0.0, h[2 * size_t(i) + 1] / cnt - mean * mean));
-    }
-    return LENIA_OK;
+    return lenia::abi_guard(bb ? &bb->ctx.message : nullptr, [&]() -> int {
+        if (!bb || !cm || !mean_luma || !stddev_luma) return LENIA_ERR_INVALID_ARG;
+        BatchContext& b = bb->ctx;
+        const int n = int(b.worlds.size());
+        static_assert(sizeof(lenia_colormap) == sizeof(lenia::ColorMapParams), "colour map layout");
+        lenia::ColorMapParams p;
+        std::memcpy(&p, cm, sizeof(p));
+        cudaError_t e = cudaMemsetAsync(b.d_stats, 0, sizeof(double) * 2 * n, b.stream);
+        if (e == cudaSuccess) {
+            lenia::activity_kernel<<<dim3(16, unsigned(n)), 256, 0, b.stream>>>(b.d_field_ptrs[b.cur], b.d_npx, p,
+                                                                                b.d_stats, n);
+            e = cudaGetLastError();
+        }
+        std::vector<double> h(2 * size_t(n));
+        if (e == cudaSuccess) e = cudaDeviceSynchronize();
+        if (e == cudaSuccess) e = cudaMemcpy(h.data(), b.d_stats, h.size() * sizeof(double), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return b.fail(LENIA_ERR_CUDA, cudaGetErrorString(e));
+        for (int i = 0; i < n; ++i) {
+            const double cnt = double(b.worlds[size_t(i)].width) * b.worlds[size_t(i)].height;
+            const double mean = h[2 * size_t(i)] / cnt;
+            mean_luma[i] = mean;
+            stddev_luma[i] = std::sqrt(std::max(0.0, h[2 * size_t(i) + 1] / cnt - mean * mean));
+        }
+        return LENIA_OK;
+    });
 }
 
 int lenia_batch_init_noise(lenia_batch* bb, uint32_t world, uint32_t seed, float init_coverage, float init_scale) {
-    if (!bb || world >= bb->ctx.worlds.size()) return LENIA_ERR_INVALID_ARG;
-    BatchContext& b = bb->ctx;
-    const lenia_world& w = b.worlds[world];
-    const lenia::InitParams ip{init_coverage, init_scale, lenia::derive_seed(seed, 0x4C454E31u), w.width, w.height};
-    cudaError_t e = lenia::launch_init_noise(b.field(int(world), b.cur), ip, b.stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(b.stream);
-    b.spectra_valid = false;
-    return e == cudaSuccess ? LENIA_OK : b.fail(LENIA_ERR_CUDA, cudaGetErrorString(e));
+    return lenia::abi_guard(bb ? &bb->ctx.message : nullptr, [&]() -> int {
+        if (!bb || world >= bb->ctx.worlds.size()) return LENIA_ERR_INVALID_ARG;
+        BatchContext& b = bb->ctx;
+        const lenia_world& w = b.worlds[world];
+        const lenia::InitParams ip{init_coverage, init_scale, lenia::derive_seed(seed, 0x4C454E31u), w.width, w.height};
+        cudaError_t e = lenia::launch_init_noise(b.field(int(world), b.cur), ip, b.stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(b.stream);
+        b.spectra_valid = false;
+        return e == cudaSuccess ? LENIA_OK : b.fail(LENIA_ERR_CUDA, cudaGetErrorString(e));
+    });
 }
 
 int lenia_batch_world_path(lenia_batch* bb, uint32_t world, uint32_t* path) {
-    if (!bb || !path || world >= bb->ctx.worlds.size()) return LENIA_ERR_INVALID_ARG;
-    *path = uint32_t(bb->ctx.path[world]);
-    return LENIA_OK;
+    return lenia::abi_guard(bb ? &bb->ctx.message : nullptr, [&]() -> int {
+        if (!bb || !path || world >= bb->ctx.worlds.size()) return LENIA_ERR_INVALID_ARG;
+        *path = uint32_t(bb->ctx.path[world]);
+        return LENIA_OK;
+    });
 }
 
 int lenia_batch_sync(lenia_batch* bb) {
-    if (!bb) return LENIA_ERR_INVALID_ARG;
-    cudaError_t e = cudaDeviceSynchronize();
-    return e == cudaSuccess ? LENIA_OK : bb->ctx.fail(LENIA_ERR_CUDA, cudaGetErrorString(e));
+    return lenia::abi_guard(bb ? &bb->ctx.message : nullptr, [&]() -> int {
+        if (!bb) return LENIA_ERR_INVALID_ARG;
+        cudaError_t e = cudaDeviceSynchronize();
+        return e == cudaSuccess ? LENIA_OK : bb->ctx.fail(LENIA_ERR_CUDA, cudaGetErrorString(e));
+    });
 }
 
-const char* lenia_batch_last_message(lenia_batch* bb) { return bb ? bb->ctx.message.c_str() : ""; }
+// NULL: the calling thread's last failed lenia_batch_create.
+const char* lenia_batch_last_message(lenia_batch* bb) {
+    return bb ? bb->ctx.message.c_str() : g_batch_create_error.c_str();
+}
 
 }  // extern "C"

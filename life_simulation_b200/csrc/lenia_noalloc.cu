@@ -12,10 +12,13 @@
 // that loads this library holds until the process exits.
 //
 // The array's host-side name is not a device address: the device address is
-// fetched once per device with cudaGetSymbolAddress (with that device
-// current) and the kernels receive that pointer.
+// fetched with cudaGetSymbolAddress (with the device current) on every call --
+// it is cheap -- and the kernels receive that pointer. If it differs from the
+// address the tables were uploaded to (the context was torn down and the
+// module reloaded, e.g. after cudaDeviceReset), the tables are rebuilt.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -24,6 +27,7 @@
 #include <vector>
 
 #include "../../include/lenia_b200.h"
+#include "abi_guard.h"
 #include "lenia_kernels.h"
 #include "lenia_module.h"
 
@@ -34,15 +38,13 @@ __device__ __align__(256) unsigned char g_noalloc_scratch[LENIA_NOALLOC_SCRATCH_
 
 constexpr int kMaxDevices = 64;
 
+// Launch shape of the compile-time-plan passes (columns / rows per CTA).
+constexpr int kColsPerCta = 4;
+constexpr int kRowsPerCta = 2;
+
 struct DeviceScratch {
-    bool ready = false;
-    unsigned char* base = nullptr;  // device address of g_noalloc_scratch
+    unsigned char* base = nullptr;  // device address of g_noalloc_scratch the tables were put in
     std::string key;                // field size + kernel shapes the tables hold
-    lenia::FftGeometry g{};
-    lenia::FastTables t{};
-    bool fast = false;
-    float2* S = nullptr;
-    float2* U = nullptr;
 };
 
 std::mutex g_mu;
@@ -60,9 +62,10 @@ int fail(int code, std::string msg) {
 
 extern "C" const char* lenia_noalloc_last_message(void) { return g_noalloc_error.c_str(); }
 
-extern "C" int lenia_fft_step_noalloc(const float* field_in, float* field_out, uint32_t width,
-                                      uint32_t height, const lenia_config* cfg,
-                                      const lenia_frame_params* fp, uint32_t seed, void* stream) {
+namespace {
+
+int step_noalloc(const float* field_in, float* field_out, uint32_t width, uint32_t height, const lenia_config* cfg,
+                 const lenia_frame_params* fp, uint32_t seed, void* stream) {
     using namespace lenia;
     if (!field_in || !field_out || !cfg || !fp)
         return fail(LENIA_ERR_INVALID_ARG, "null argument");
@@ -70,12 +73,13 @@ extern "C" int lenia_fft_step_noalloc(const float* field_in, float* field_out, u
     // The row pass stages the field with 16-byte asynchronous copies.
     if ((reinterpret_cast<uintptr_t>(field_in) | reinterpret_cast<uintptr_t>(field_out)) & 15u)
         return fail(LENIA_ERR_INVALID_ARG, "field_in and field_out must be 16-byte aligned");
-    if (!(fp->growth_sigma != 0.0f)) return fail(LENIA_ERR_INVALID_ARG, "growth_sigma must be nonzero");
     FftPlan prow{}, pcol{};
     if (width < 2 || (width & 1u) || height < 1 || !fft_plan(int(width / 2), prow) || !fft_plan(int(height), pcol))
         return fail(LENIA_ERR_UNSUPPORTED,
                     "field size needs an even width and sizes with factors 2, 3, 5 only");
-    if (cfg->num_kernels > 4) return fail(LENIA_ERR_UNSUPPORTED, "at most 4 kernels");
+    // More than 4 kernels are truncated to the first 4, as the module's setup
+    // does (Lenia.cpp:225-230).
+    const uint32_t num_kernels = std::min<uint32_t>(cfg->num_kernels, 4u);
 
     // Kernels: the config's, or one implicit kernel (Lenia.cpp:503-512).
     struct K {
@@ -83,20 +87,28 @@ extern "C" int lenia_fft_step_noalloc(const float* field_in, float* field_out, u
         std::vector<float> betas;
     };
     std::vector<K> ks;
-    for (uint32_t i = 0; i < cfg->num_kernels; ++i) {
+    for (uint32_t i = 0; i < num_kernels; ++i) {
         const lenia_kernel_def& d = cfg->kernels[i];
         if (d.num_betas > 8) return fail(LENIA_ERR_UNSUPPORTED, "a kernel has more than 8 betas");
+        if (!(d.sigma != 0.0f)) return fail(LENIA_ERR_INVALID_ARG, "a kernel's sigma must be nonzero");
         K k{d.radius_scale, d.mu, d.sigma, d.weight, std::vector<float>(d.betas, d.betas + d.num_betas)};
         if (k.betas.empty()) k.betas.push_back(1.0f);
         ks.push_back(std::move(k));
     }
-    if (ks.empty()) ks.push_back(K{1.0f, fp->growth_mu, fp->growth_sigma, 1.0f, {1.0f}});
+    if (ks.empty()) {
+        if (!(fp->growth_sigma != 0.0f)) return fail(LENIA_ERR_INVALID_ARG, "growth_sigma must be nonzero");
+        ks.push_back(K{1.0f, fp->growth_mu, fp->growth_sigma, 1.0f, {1.0f}});
+    }
     const int nk = int(ks.size());
     const uint32_t radius = cfg->radius;
 
     const int M = int(width / 2), H = int(height), Hh = H / 2 + 1;
     FastPlan cf, ri;
-    const bool fast = fast_col_plan(H, cf) && fast_row_plan(M, ri) && M % kSpectralBlock == 0;
+    // Compile-time-plan kernels at 4 columns and 2 rows per CTA where the
+    // catalogue has the size and that launch shape fits; else the
+    // runtime-plan kernels.
+    const bool fast = fast_col_plan(H, cf) && fast_row_plan(M, ri) && M % kSpectralBlock == 0 &&
+                      fast_shapes_supported(H, M, kColsPerCta, kRowsPerCta);
 
     // Scratch layout (256-byte aligned regions).
     const size_t spec = size_t(M) * H * sizeof(float2);
@@ -142,12 +154,12 @@ extern "C" int lenia_fft_step_noalloc(const float* field_in, float* field_out, u
 
     std::lock_guard<std::mutex> lock(g_mu);
     DeviceScratch& d = g_dev[dev];
-    if (!d.ready) {
+    {
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess || !p) return fail(LENIA_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+        if (p != d.base) d.key.clear();  // a new module instance: its array holds no tables yet
         d.base = static_cast<unsigned char*>(p);
-        d.ready = true;
     }
 
     // Tables depend on the field size and the kernel shapes only; rebuild and
@@ -248,9 +260,9 @@ extern "C" int lenia_fft_step_noalloc(const float* field_in, float* field_out, u
 
     cudaError_t e;
     if (fast) {
-        e = launch_row_fast(g, t, 2, nullptr, field_in, nullptr, S, p, 0, s);
-        if (e == cudaSuccess) e = launch_col_fast(g, t, 4, S, U, s);
-        if (e == cudaSuccess) e = launch_row_fast(g, t, 2, U, field_in, field_out, nullptr, p, nk, s);
+        e = launch_row_fast(g, t, kRowsPerCta, nullptr, field_in, nullptr, S, p, 0, s);
+        if (e == cudaSuccess) e = launch_col_fast(g, t, kColsPerCta, S, U, s);
+        if (e == cudaSuccess) e = launch_row_fast(g, t, kRowsPerCta, U, field_in, field_out, nullptr, p, nk, s);
     } else {
         e = launch_row_r2c(g, field_in, S, s);
         if (e == cudaSuccess) e = launch_col_conv(g, S, U, s);
@@ -259,4 +271,15 @@ extern "C" int lenia_fft_step_noalloc(const float* field_in, float* field_out, u
     if (e != cudaSuccess) return fail(LENIA_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
     g_noalloc_error.clear();
     return LENIA_OK;
+}
+
+}  // namespace
+
+// No C++ exception leaves the C ABI: a failed host allocation (the kernel
+// spectra are built in host vectors) or any other exception becomes a status.
+extern "C" int lenia_fft_step_noalloc(const float* field_in, float* field_out, uint32_t width,
+                                      uint32_t height, const lenia_config* cfg,
+                                      const lenia_frame_params* fp, uint32_t seed, void* stream) {
+    return lenia::abi_guard(&g_noalloc_error,
+                            [&] { return step_noalloc(field_in, field_out, width, height, cfg, fp, seed, stream); });
 }

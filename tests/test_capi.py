@@ -11,7 +11,7 @@ import subprocess
 import pytest
 
 import life_simulation_b200 as lb
-from tests.conftest import ROOT
+from tests.conftest import GOLDEN, ROOT, reference_preset
 
 HEADER = os.path.join(ROOT, "include", "lenia_b200.h")
 
@@ -47,10 +47,7 @@ def test_status_strings():
 
 
 def preset(name):
-    p = os.path.join("/root/reference/Presets", name)
-    if not os.path.exists(p):
-        pytest.skip("reference presets not present")
-    return json.load(open(p))["modules"][0]["params"]
+    return reference_preset(name.replace(".json", ""))[0]
 
 
 def test_inspect_direct_default():
@@ -111,7 +108,7 @@ def test_inspect_reference_presets():
         1024, 512, lb.CONV_FFT, 3, 24)
     r = lb.inspect(preset("lenia_basic.json"), 768, 768)
     assert (r["conv_mode"], r["radius"]) == (lb.CONV_DIRECT, 13)
-    r = lb.inspect(preset("lenia_orbium.json"), 1280, 720, base_dir="/root/reference")
+    r = lb.inspect(preset("lenia_orbium.json"), 1280, 720, base_dir=GOLDEN)
     assert r["use_stamp_init"] == 1 and r["radius"] == 13
 
 
@@ -173,3 +170,37 @@ def test_inspect_reports_the_direct_radius_limit_like_setup():
     # A non-power-of-two size falls back to direct, where R = 40 is refused.
     with pytest.raises(lb.LeniaError, match="radius <= 32"):
         lb.inspect({"radius": 40, "convMode": "fft"}, 250, 256)
+
+
+_ALLOC_FAILURE_CHILD = r"""
+import ctypes, resource, sys
+sys.path.insert(0, sys.argv[1])
+import life_simulation_b200 as lb
+L = lb.load_library()
+cfg = lb.config_from_params({"convMode": "fft", "radius": 9})
+fp = lb.make_frame_params(growth_sigma=0.02)
+# Cap the address space a little above what the process maps now, so the
+# call's host tables (a twiddle table of width/2 entries: 1 GiB here) cannot
+# be allocated.
+soft, hard = resource.getrlimit(resource.RLIMIT_AS)
+used = int(open("/proc/self/statm").read().split()[0]) * resource.getpagesize()
+resource.setrlimit(resource.RLIMIT_AS, (used + (256 << 20), hard))
+w, h = 1 << 28, 1
+# Aligned, distinct, never dereferenced on the host (the call fails before
+# any device work).
+rc = L.lenia_fft_step_noalloc(ctypes.c_void_p(1 << 20), ctypes.c_void_p(2 << 20), w, h, ctypes.byref(cfg),
+                              ctypes.byref(fp), 1, None)
+print(rc, L.lenia_noalloc_last_message().decode())
+"""
+
+
+def test_host_allocation_failure_is_a_status_not_an_exception():
+    # A C++ std::bad_alloc inside an entry point must come back as a status
+    # code with a message, never unwind through the C ABI (which would
+    # abort the process). The child process caps its address space so the
+    # entry point's host tables cannot be allocated.
+    r = subprocess.run([os.sys.executable, "-c", _ALLOC_FAILURE_CHILD, ROOT], capture_output=True, text=True,
+                       timeout=120)
+    assert r.returncode == 0, r.stderr[-2000:]
+    rc, msg = r.stdout.strip().split(" ", 1)
+    assert int(rc) == -3 and "host allocation failed" in msg, r.stdout

@@ -16,6 +16,7 @@ import pytest
 
 from oracle import lenia_oracle as lo
 from oracle.lenia_oracle import OracleLenia, RefLenia
+from tests.conftest import orbium_organism, reference_preset
 
 
 def _organism_for(params):
@@ -178,12 +179,8 @@ def test_orbium_glides_and_survives_400_frames():
     # with its own R, T, mu, sigma) survives 400 frames as a glider
     # (docs/specs/phase11_organisms.md:74-81). One stamp on a 96x96 torus,
     # FP32 restatement: the mass holds and the pattern moves.
-    ref = "/root/reference"
-    preset = os.path.join(ref, "Presets", "lenia_orbium.json")
-    if not os.path.exists(preset):
-        pytest.skip("reference presets not present")
-    params = json.load(open(preset))["modules"][0]["params"]
-    d = json.load(open(os.path.join(ref, params["organism"])))
+    params = reference_preset("lenia_orbium")[0]
+    d = orbium_organism()
     org = lo.Organism(np.asarray(d["cells"], np.float32), d["R"], d["T"], d["mu"], d["sigma"])
     p = dict(params, simWidth=96, simHeight=96, stampCount=1, stampRotate=False)
     o = OracleLenia(p, 96, 96, "ref32", organism=org)
