@@ -69,3 +69,44 @@ def test_batch_auto_prefers_direct_for_small_radius():
     assert b.path(0) == lb.CONV_DIRECT
     assert b.path(1) == lb.CONV_FFT
     b.close()
+
+
+def test_sweep_batch_worlds_vs_fp64_oracle():
+    """The benchmarked 512-world sweep batch (the autotuner's path choice per
+    world): one world of each size class compared with the FP64 oracle
+    directly. Every step the sampled worlds are set to a state, the whole
+    batch steps once, and each sampled world must be within 1e-5 of one FP64
+    step of the oracle from the same state (the plain path's per-step bound);
+    the states are the batch's own trajectory."""
+    from life_simulation_b200 import workloads as wl
+    from oracle.lenia_oracle import OracleLenia
+
+    params, inits = wl.sweep512()
+    worlds = [lb.make_world(**p) for p in params]
+    b = lb.LeniaBatch(worlds, lb.BATCH_AUTO)
+    for i, a in enumerate(inits):
+        b.upload(i, a)
+    sample = []
+    for size in [(128, 128), (256, 256), (384, 216), (512, 512)]:
+        sample.append(next(i for i, w in enumerate(worlds) if (w.width, w.height) == size))
+    oracles = {}
+    for i in sample:
+        w = worlds[i]
+        conv = "fft" if b.path(i) == lb.CONV_FFT else "direct"
+        o = OracleLenia(lb.single_world_params(w, conv), w.width, w.height, "f64")
+        o.reset(w.seed)
+        o.set_initial_field(inits[i])
+        o.encode(0)  # builds the kernels; the state is replaced below
+        oracles[i] = o
+    b.step(3)  # into the live phase
+    worst = {i: 0.0 for i in sample}
+    for s in range(8):
+        states = {i: b.field(i) for i in sample}
+        b.step(1)
+        for i in sample:
+            o = oracles[i]
+            o.state = states[i].astype(np.float64)
+            o.step_once(o.frame_params(), 0, 3 + s, 3 + s)
+            worst[i] = max(worst[i], float(np.abs(b.field(i) - o.state).max()))
+    assert max(worst.values()) <= 1e-5, {(worlds[i].width, worlds[i].height, b.path(i)): e for i, e in worst.items()}
+    b.close()
