@@ -13,9 +13,14 @@ pixels x steps; ``value`` is whole-job Mpixel-steps/s.
   collective on the data path; weak scaling). Before the warm-up the launch
   shapes of the two passes are chosen under these same conditions
   (lenia_set_tuning; --keep-tuning keeps the setup autotuner's).
-* e2e: the same metric through the C ABI with host buffers: per step
-  lenia_upload (pinned host -> device), lenia_step, lenia_download (device ->
-  pinned host), timed by CUDA events on the context stream.
+* e2e: the same metric through the C ABI with host buffers: every step
+  copies its whole input field in from pinned host memory and its whole
+  result out to pinned host memory. The copies run on their own streams
+  through device staging buffers (lenia_upload_device / lenia_step /
+  lenia_download_device on the step's stream), so a step overlaps the next
+  input's copy and the previous result's copy; CUDA events from the first
+  copy in to the last copy out. e2e.serial: lenia_upload, lenia_step,
+  lenia_download in turn.
 * roofline: the dominant kernel's algorithmic bytes per launch (HBM-bound
   figures of the spectral path, per pixel: column pass 4 + 2K + 4K, row
   growth pass 4K + 4 + 4 + 4) over its mean launch duration, timed by CUDA
@@ -31,10 +36,16 @@ pixels x steps; ``value`` is whole-job Mpixel-steps/s.
   mode 1, T=64, checkpoints every 8): device time of the forward rollout and of the
   backward (recomputation included), CUDA events on the launching stream
   with an L2 flush before each; ratio = backward / forward.
-* tc: 4096x4096, 3 kernels R=32, 64 steps per arithmetic of the column DFT
-  stages (fp32 CUDA cores, fp16x3 / bf16x3 split-precision tensor cores);
-  per-step device time, the column pass's HBM roofline and tensor FLOP rate
-  (a radix-16 stage as a real 32x32 GEMM: 128 FLOP per point, x3 hi/lo).
+* sweep (one GPU): the 512-world sweep (128 each of 128^2, 256^2, 384x216,
+  512^2; R 8..32), batched against the plain one-context-per-world loop;
+  Mpixel-steps/s of both, the speed-up and the per-readback activity.
+* tc (one GPU): 4096x4096, 3 kernels R=32, 64 steps per arithmetic of the
+  column DFT stages (fp32 CUDA cores, fp16x3 / bf16x3 split-precision tensor
+  cores); per-step device time, the column pass's HBM roofline and tensor
+  FLOP rate (a radix-16 stage as a real 32x32 GEMM: 128 FLOP per point, x3
+  hi/lo), and each one's max / RMS error against the FP64 oracle.
+* cpu_baseline_fft_1024x512: the reference's own FFT path (85 passes per
+  substep) compiled for the CPU, whole 1024x512 field, all host threads.
 * library_fft_baseline: the same step from torch.fft (cuFFT) and torch ops
   in one CUDA graph, same flush protocol: a library comparator.
 * published_config / published_direct_config: 1024x512, 3 kernels R=24 (FFT)
@@ -63,9 +74,23 @@ METRIC = "Lenia Mpixel-steps/s (FFT, 3 kernels, 1080p)"
 UNIT = "Mpixel-steps/s"
 WORKLOAD = "fft3_1080p"
 FALLBACK_HBM_GBS = 6650.0
-# dram__bytes_read.sum + dram__bytes_write.sum per launch from one ncu
-# capture of the default workload (profiles/lenia_fft_step_1080p_k3.md).
-NCU_TRAFFIC_BYTES = {"row_growth": 33_260_800 + 8_704, "column": 14_577_152 + 0}
+# DRAM traffic per launch (dram__bytes_read.sum + dram__bytes_write.sum) of
+# the step's kernels, as one ncu capture of this workload measured it, with
+# the capture's command: written beside the ncu summaries when a capture is
+# taken. Without it, roofline.traffic is null.
+TRAFFIC_FILE = os.path.join(ROOT, "profiles", "ncu_dram_traffic.json")
+
+
+def captured_traffic(kernel: str, workload: str):
+    """(bytes per launch, source) from the capture file, or (None, None)."""
+    try:
+        d = json.load(open(TRAFFIC_FILE))
+    except (OSError, ValueError):
+        return None, None
+    k = d.get("kernels", {}).get(kernel)
+    if not k or d.get("workload") != workload:
+        return None, None
+    return int(k["dram_bytes_per_launch"]), f"ncu capture: {d.get('command')} ({d.get('note', '')})"
 
 
 def parse_args():
@@ -85,8 +110,11 @@ def parse_args():
     ap.add_argument("--adjoint-reps", type=int, default=5)
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-library-baseline", action="store_true")
+    ap.add_argument("--no-sweep", action="store_true", help="skip the 512-world sweep in the step line")
+    ap.add_argument("--no-tc", action="store_true", help="skip the 4096^2 tensor-core comparison in the step line")
     ap.add_argument("--launch-shape", default=None,
-                    help="columns,rows per CTA of the two passes, e.g. 4,4p (p: pipelined rows); "
+                    help="columns,rows per CTA of the two passes, e.g. 4,4p (p: pipelined rows; "
+                         "h after the columns: half-thread column pass); "
                          "skips the shape search")
     ap.add_argument("--keep-tuning", action="store_true",
                     help="keep the setup autotuner's launch shapes instead of choosing them under the "
@@ -342,6 +370,40 @@ def library_fft_baseline(params, w, h, init, steps: int = 50, warmup: int = 5) -
             "ms_per_step": ms, "value": w * h / (ms / 1e3) / 1e6, "unit": UNIT, "steps": steps}
 
 
+def cpu_baseline_fft_1024x512(seconds: float = 8.0) -> dict:
+    """The reference's own FFT path (radix-2 Stockham passes, 85 per substep
+    at K=3: Modules/FieldModules/Lenia.cpp:576-643, Shaders/Common/
+    FFT.metal:65-177) compiled for the CPU, on the whole 1024x512 field of
+    the multi-kernel workload (3 kernels R=24, the reference's Gaussian-shell
+    core), all host threads: the like-for-like CPU figure for the spectral
+    path, where 1080p makes the reference fall back to direct convolution."""
+    from life_simulation_b200 import workloads as wl
+    from oracle.lenia_oracle import RefLenia
+
+    if not RefLenia.available():
+        return {"value": None, "error": "oracle/_ref (compiled reference) not built"}
+    p = wl.fft3_params(1024, 512)
+    p.pop("kernelCore")
+    p.pop("fftAnySize")
+    r = RefLenia(p, 1024, 512)
+    r.reset(2)
+    r.set_initial_field(wl.patches(1024, 512, 20, 96, seed=2))
+    r.encode(0, 1)  # init pass + kernel spectra + one substep (warm-up)
+    p0 = r.pass_count()
+    steps, t0 = 0, time.perf_counter()
+    while True:
+        r.encode(1 + steps, 1)
+        steps += 1
+        el = time.perf_counter() - t0
+        if el >= seconds or steps >= 200:
+            break
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return {"value": 1024 * 512 * steps / el / 1e6, "unit": UNIT, "cores": cores, "kind": "reference",
+            "passes_per_substep": (r.pass_count() - p0) / steps,
+            "sample": f"whole 1024x512 field, 3 kernels R=24 (Gaussian shell), convMode fft: {steps} "
+                      f"substeps in {el:.1f} s"}
+
+
 def cpu_baseline(params, w, h, init, seconds):
     from oracle.lenia_oracle import RefLenia
     if RefLenia.available():
@@ -489,12 +551,13 @@ def run_b200(args):
     shape, chosen_by = m.tuning(), "setup autotuner"
     if shape != (0, 0) and args.launch_shape:
         c, r = args.launch_shape.split(",")
-        shape = (int(c), int(r.rstrip("p")) | (lb.ROWS_PIPELINED if r.endswith("p") else 0))
+        shape = (int(c.rstrip("h")) | (lb.COLS_HALF_THREADS if c.endswith("h") else 0),
+                 int(r.rstrip("p")) | (lb.ROWS_PIPELINED if r.endswith("p") else 0))
         m.set_tuning(*shape)
         chosen_by = "--launch-shape"
     elif shape != (0, 0) and not args.keep_tuning:
         best = None
-        for c in (8, 4, 2):
+        for c in (8, 4, 2, 4 | lb.COLS_HALF_THREADS):
             for r in (4, 2, 1, 4 | lb.ROWS_PIPELINED, 2 | lb.ROWS_PIPELINED, 1 | lb.ROWS_PIPELINED):
                 try:
                     m.set_tuning(c, r)
@@ -559,30 +622,77 @@ def run_b200(args):
     render_line = {"what": "one substep + the RGBA16F colour layer at the sim size per frame, L2 flushed",
                    "separate_ms": frame_ms["separate"], "fused_ms": frame_ms["fused"]}
 
-    # End to end through the C ABI with pinned host buffers.
+    # End to end through the C ABI with pinned host buffers, two ways.
+    # serial: per step lenia_upload (pinned host -> field), lenia_step,
+    # lenia_download (field -> pinned host), each call waiting for the last.
+    # pipelined (the e2e figure): every step still copies its whole input in
+    # from pinned host memory and its whole result out, but the copies run on
+    # their own streams into / out of device staging buffers, so step i's
+    # host->device copy overlaps step i-1's compute and step i-2's
+    # device->host copy (PCIe moves both directions at once); the staged
+    # field enters and leaves the context by lenia_upload_device /
+    # lenia_download_device on the step's stream. Timed by CUDA events from
+    # the first copy in to the last copy out.
     e2e_steps = args.e2e_steps or max(10, args.steps // 4)
-    host_in = torch.empty((h, w), dtype=torch.float32, pin_memory=True).numpy()
-    host_out = torch.empty((h, w), dtype=torch.float32, pin_memory=True).numpy()
-    host_in[:] = m.field()
+    host_in = [torch.empty((h, w), dtype=torch.float32, pin_memory=True) for _ in range(2)]
+    host_out = [torch.empty((h, w), dtype=torch.float32, pin_memory=True) for _ in range(2)]
+    start_field = torch.from_numpy(m.field())
+    for x in host_in:
+        x.copy_(start_field)
     ctx_stream = torch.cuda.ExternalStream(m.stream())
     barrier()
-    e2e_ms = 0.0
+    serial_ms = 0.0
     for i in range(e2e_steps):
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         fp.frame_index = fp.audio_frame = 100000 + i
         a.record(ctx_stream)
-        m.upload(host_in)
+        m.upload(host_in[0].numpy())
         m.step(fp, 1, None)
-        m.download_into(host_out)
+        m.download_into(host_out[0].numpy())
         b.record(ctx_stream)
         b.synchronize()
-        e2e_ms += a.elapsed_time(b)
-        host_in, host_out = host_out, host_in
+        serial_ms += a.elapsed_time(b)
+    d_in = [torch.empty((h, w), dtype=torch.float32, device="cuda") for _ in range(2)]
+    d_out = [torch.empty((h, w), dtype=torch.float32, device="cuda") for _ in range(2)]
+    s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
+    ev_in = [torch.cuda.Event() for _ in range(e2e_steps)]
+    ev_step = [torch.cuda.Event() for _ in range(e2e_steps)]
+    ev_out = [torch.cuda.Event() for _ in range(e2e_steps)]
+    t_a, t_b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    t_a.record(s_in)
+    for i in range(e2e_steps):
+        k = i % 2
+        with torch.cuda.stream(s_in):
+            if i >= 2:
+                s_in.wait_event(ev_step[i - 2])  # staging buffer k consumed by step i-2
+            d_in[k].copy_(host_in[k], non_blocking=True)
+            ev_in[i].record(s_in)
+        stream.wait_event(ev_in[i])
+        if i >= 2:
+            stream.wait_event(ev_out[i - 2])  # result buffer k copied out
+        fp.frame_index = fp.audio_frame = 200000 + i
+        m.upload_device(d_in[k].data_ptr(), sh)
+        m.step(fp, 1, sh)
+        m.download_device(d_out[k].data_ptr(), sh)
+        ev_step[i].record(stream)
+        with torch.cuda.stream(s_out):
+            s_out.wait_event(ev_step[i])
+            host_out[k].copy_(d_out[k], non_blocking=True)
+            ev_out[i].record(s_out)
+    s_out.wait_event(ev_out[-1])
+    t_b.record(s_out)
+    barrier()
+    e2e_ms = t_a.elapsed_time(t_b)
+    # The pipelined results are the real steps: the last one equals the
+    # context's field.
+    e2e_ok = bool(np.array_equal(host_out[(e2e_steps - 1) % 2].numpy(), m.field()))
     if world > 1:
-        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
+        t = torch.tensor([e2e_ms, serial_ms], device="cuda", dtype=torch.float64)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+        e2e_ms, serial_ms = float(t[0].item()), float(t[1].item())
     e2e_value = world * w * h * e2e_steps / (e2e_ms / 1e3) / 1e6
+    e2e_serial = world * w * h * e2e_steps / (serial_ms / 1e3) / 1e6
 
     # Roofline of the dominant kernel (HBM bound).
     K = len(params.get("kernels", [])) or 1
@@ -603,7 +713,9 @@ def run_b200(args):
     mean_step_ms = total_ms / args.steps
     line = base_line(args, world, args.steps, args.warmup, w, h, params)
     if shape != (0, 0):
-        line["config"]["launch_shape"] = {"cols_per_cta": shape[0], "rows_per_cta": shape[1] & 0xFF,
+        line["config"]["launch_shape"] = {"cols_per_cta": shape[0] & 0xF,
+                                          "cols_half_threads": bool(shape[0] & lb.COLS_HALF_THREADS),
+                                          "rows_per_cta": shape[1] & 0xFF,
                                           "rows_pipelined": bool(shape[1] & lb.ROWS_PIPELINED),
                                           "chosen_by": chosen_by}
     if direct_flops is not None:
@@ -614,9 +726,10 @@ def run_b200(args):
                     "frac": tflops / fp32_peak, "traffic": None, "algorithmic_flops_per_launch": direct_flops,
                     "launch_ms": launch_ms}
     else:
+        traffic, traffic_source = captured_traffic(dom, args.workload)
         roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                     "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak,
-                    "traffic": NCU_TRAFFIC_BYTES.get(dom),
+                    "traffic": traffic, "traffic_source": traffic_source,
                     "algorithmic_bytes_per_launch": bytes_px[dom] * w * h,
                     "launch_ms": launch_ms,
                     "step": {"bytes": step_bytes, "achieved": step_bytes / (mean_step_ms / 1e3) / 1e9,
@@ -624,7 +737,11 @@ def run_b200(args):
     line.update({
         "value": value, "ms_per_step": mean_step_ms,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(w * h * 4),
-                "d2h_bytes_per_step": int(w * h * 4), "steps": e2e_steps},
+                "d2h_bytes_per_step": int(w * h * 4), "steps": e2e_steps,
+                "how": "pipelined: pinned host -> staging (copy stream), lenia_upload_device + lenia_step + "
+                       "lenia_download_device (step stream), staging -> pinned host (copy stream)",
+                "last_result_equals_field": e2e_ok,
+                "serial": {"value": e2e_serial, "how": "lenia_upload, lenia_step, lenia_download in turn"}},
         "gpu_launches": int(launches),
         "roofline": roofline,
         "phases_ms_per_step": {k: v["ms"] / prof_steps for k, v in phases.items()},
@@ -639,11 +756,19 @@ def run_b200(args):
     if rank == 0 and world == 1 and args.workload == WORKLOAD:
         line["published_config"] = published_config_bench()
         line["published_direct_config"] = published_direct_bench()
+    if rank == 0 and world == 1 and not args.no_sweep:
+        line["sweep"] = sweep_bench(args.plain_steps)
+    if rank == 0 and world == 1 and not args.no_tc:
+        line["tc"] = tc_bench(error_check=not args.no_cpu_baseline)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_baseline(params, w, h, init, args.cpu_seconds)
         except Exception as e:  # the oracle is optional here; the GPU number stands
             line["cpu_baseline"] = {"value": None, "error": str(e)}
+        try:
+            line["cpu_baseline_fft_1024x512"] = cpu_baseline_fft_1024x512()
+        except Exception as e:
+            line["cpu_baseline_fft_1024x512"] = {"value": None, "error": str(e)}
         try:
             line["accuracy_vs_fp64"] = accuracy_vs_fp64(params, w, h, init)
         except Exception as e:
@@ -723,20 +848,21 @@ def run_adjoint(args):
     return 0
 
 
-def run_tc(args):
-    """4096x4096, 3 kernels R=32: the column DFT stages on the CUDA cores (FP32) and
-    on the tensor cores (FP16 / BF16 hi/lo, FP32 accumulation)."""
+def tc_bench(warmup: int = 3, steps: int = 64, error_check: bool = True) -> dict:
+    """4096x4096, 3 kernels R=32: the column DFT stages on the CUDA cores (FP32)
+    and on the tensor cores (FP16 / BF16 hi/lo, FP32 accumulation): per
+    precision the device time per step, the column pass's HBM roofline and
+    tensor FLOP rate, and (error_check) max / RMS |A - A_fp64| of one step
+    from the same field against the FP64 oracle."""
     import torch
 
     import life_simulation_b200 as lb
     from life_simulation_b200 import workloads as wl
 
-    torch.cuda.set_device(0)
     w = h = 4096
-    K, steps = 3, 64
+    K = 3
     init = wl.patches(w, h, 40, 256, seed=2)
     stream = torch.cuda.Stream()
-    torch.cuda.set_stream(stream)
     sh = stream.cuda_stream
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     peak, peak_kind = measured_peaks()
@@ -745,6 +871,7 @@ def run_tc(args):
     # x 128 FLOP (real 32x32 GEMM per 16 points) x 3 (hi/lo), per column.
     tc_flops = (1 + K) * 3 * h * 128 * 3 * (w // 2)
     res = {}
+    state = None  # the field the error check steps from (after the FP32 run's warm-up)
     for prec in ("fp32", "fp16x3", "bf16x3"):
         p = wl.fft3_params(w, h)
         p["radius"] = 32
@@ -753,14 +880,15 @@ def run_tc(args):
         m.reset(2)
         m.upload(init)
         fp = m.frame_params(0)
-        for i in range(max(3, args.warmup)):
+        for i in range(max(3, warmup)):
             fp.frame_index = fp.audio_frame = i
             m.step(fp, 1, sh)
         torch.cuda.synchronize()
         m.profile(True)
         evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
         for i in range(steps):
-            flush.zero_()
+            with torch.cuda.stream(stream):
+                flush.zero_()
             fp.frame_index = fp.audio_frame = 100 + i
             evs[i][0].record(stream)
             m.step(fp, 1, sh)
@@ -777,53 +905,60 @@ def run_tc(args):
              "fft_precision": m.info()["fft_precision"]}
         if prec != "fp32":
             r["column_tensor_tflops"] = tc_flops / (col_ms / 1e3) / 1e12
+        if error_check:
+            if state is None:
+                state = m.field()
+            m.upload(state)
+            fp.frame_index = fp.audio_frame = 0
+            m.step(fp, 1, sh)
+            torch.cuda.synchronize()
+            r["_next"] = m.field()
         res[prec] = r
         m.close()
-    print(json.dumps({
-        "metric": "Lenia Mpixel-steps/s, 4096x4096 K=3 R=32: column DFT stages FP32 CUDA cores vs split-precision tensor cores",
-        "unit": UNIT, "value": res["fp32"]["mpx_steps_s"], "higher_is_better": True, "n_gpus": 1, "steps": steps,
-        "dtype": "f32 / fp16x3 / bf16x3", "data": "synthetic",
-        "config": {"workload": "4096x4096, 3 kernels R=32 (fft3 peaks/mu/sigma/h), 40 patches of 256x256 (seed 2)",
-                   "l2": "256 MiB write between steps"},
-        "peak_hbm_gbs": peak, "peak_source": peak_kind, "column_bytes_per_launch": col_bytes,
-        "column_tensor_flops_per_launch": tc_flops, "precisions": res}))
+    if error_check:
+        from oracle import lenia_oracle as lo
+        p = wl.fft3_params(w, h)
+        p["radius"] = 32
+        o = lo.OracleLenia(p, w, h, "f64")
+        o.reset(2)
+        o.set_initial_field(state)
+        o.encode(0)  # builds the kernels; its state is replaced below
+        o.state = state.astype(np.float64)
+        o.step_once(o.frame_params(), lo.pcg_hash(o.seed_), 0, 0)
+        for prec, r in res.items():
+            d = r.pop("_next").astype(np.float64) - o.state
+            r["max_err_vs_fp64"] = float(np.abs(d).max())
+            r["rms_err_vs_fp64"] = float(np.sqrt(np.mean(d * d)))
+    return {"workload": "4096x4096, 3 kernels R=32 (fft3 peaks/mu/sigma/h), 40 patches of 256x256 (seed 2)",
+            "steps": steps, "l2": "256 MiB write between steps", "peak_hbm_gbs": peak, "peak_source": peak_kind,
+            "column_bytes_per_launch": col_bytes, "column_tensor_flops_per_launch": tc_flops,
+            "error": "one step from the same field (after the FP32 warm-up) vs the FP64 oracle",
+            "precisions": res}
+
+
+def run_tc(args):
+    import torch
+
+    torch.cuda.set_device(0)
+    r = tc_bench(args.warmup)
+    line = {"metric": "Lenia Mpixel-steps/s, 4096x4096 K=3 R=32: column DFT stages FP32 CUDA cores vs "
+                      "split-precision tensor cores",
+            "unit": UNIT, "value": r["precisions"]["fp32"]["mpx_steps_s"], "higher_is_better": True, "n_gpus": 1,
+            "dtype": "f32 / fp16x3 / bf16x3", "data": "synthetic", "config": {"workload": r["workload"]}}
+    line.update(r)
+    print(json.dumps(line))
     return 0
 
 
-def run_sweep(args):
-    """The 512-world sweep: 512 worlds of mixed sizes, 240 substeps with the
-    activity readback every 60, batched (one graph per 60 substeps) against
-    the plain form (one context per world, worlds stepped one at a time)."""
+def sweep_batched(worlds, inits):
+    """The 512-world sweep's batched form on this GPU: the batch's graphs
+    replay 4 x 60 substeps with the activity readback after each (the lab's
+    luma statistic per world). Returns (wall seconds, per-readback activity,
+    path per world)."""
     import torch
 
     import life_simulation_b200 as lb
-    from life_simulation_b200 import workloads as wl
-    from life_simulation_b200.shard import loads, partition, world_cost
     from life_simulation_b200.sweep import is_alive
-
-    rank, world, local = dist_env()
-    if world > 1:
-        import datetime
-
-        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    torch.cuda.set_device(local)
-    specs, inits = wl.sweep512()
-    px_all = sum(s["width"] * s["height"] for s in specs)
-    # Several GPUs: each rank steps its cost-balanced share of the worlds as
-    # one batch; nothing crosses between GPUs until the final timing.
-    costs = [world_cost(s["width"], s["height"], s["radius"]) for s in specs]
-    shares = partition(costs, world)
-    mine = shares[rank]
-    specs = [specs[i] for i in mine]
-    inits = [inits[i] for i in mine]
-    worlds = [lb.make_world(s["width"], s["height"], s["radius"], s["mu"], s["sigma"], s["dt"], 0,
-                            seed=s["seed"]) for s in specs]
-    px = sum(w.width * w.height for w in worlds)
-
-    def barrier():
-        torch.cuda.synchronize()
-        if world > 1:
-            torch.distributed.barrier()
 
     b = lb.LeniaBatch(worlds, lb.BATCH_AUTO)
     for i, a in enumerate(inits):
@@ -835,42 +970,45 @@ def run_sweep(args):
     b.step(0)
     b.sync()
     cm = lb.colormap_from_params({})
-    barrier()
+    torch.cuda.synchronize()
     t0 = time.perf_counter()
     acts = []
     for _ in range(4):
         b.step(60)
-        acts.append(b.activity(cm))  # synchronising readback: the lab's luma activity per world
-    batched_s = time.perf_counter() - t0
+        acts.append(b.activity(cm))  # synchronising readback
+    seconds = time.perf_counter() - t0
     # Per readback: the worlds' mean luma and luma variance, averaged over
-    # this rank's worlds, and how many pass the lab's alive rule.
+    # the worlds, and how many pass the lab's alive rule.
     activity = [{"step": 60 * (j + 1), "mean_luma": float(mean.mean()), "mean_var_luma": float((std * std).mean()),
                  "alive": sum(1 for x, y in zip(mean, std) if is_alive(float(x), float(y)))}
                 for j, (mean, std) in enumerate(acts)]
     paths = [b.path(i) for i in range(len(worlds))]
     b.close()
-    if world > 1:
-        t = torch.tensor([batched_s], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        batched_s = float(t.item())
-        n_direct = torch.tensor([paths.count(lb.CONV_DIRECT)], device="cuda")
-        torch.distributed.all_reduce(n_direct)
-        barrier()
-        torch.distributed.destroy_process_group()
-        if rank == 0:
-            batched = px_all * 240 / batched_s / 1e6
-            print(json.dumps({
-                "metric": "Lenia Mpixel-steps/s, 512-world sweep (batched, worlds sharded over GPUs)",
-                "unit": UNIT, "value": batched, "n_gpus": world, "scaling": "strong", "worlds": 512,
-                "pixels_per_step": px_all, "steps": 240, "direct_worlds": int(n_direct.item()),
-                "shares": [len(x) for x in shares],
-                "estimated_load_ratio": max(loads(costs, shares)) / min(loads(costs, shares)),
-                "timing": "wall clock incl. 4 activity readbacks, max over ranks; worlds assigned "
-                          "largest estimated cost first to the least-loaded rank"}))
-        return 0
-    # Plain form: one context per world (its own kernel launches), the same
-    # path per world, worlds stepped one after another for a sample of steps.
-    plain_steps = args.plain_steps
+    return seconds, activity, paths
+
+
+def sweep_worlds(specs):
+    import life_simulation_b200 as lb
+
+    return [lb.make_world(s["width"], s["height"], s["radius"], s["mu"], s["sigma"], s["dt"], 0, seed=s["seed"])
+            for s in specs]
+
+
+def sweep_bench(plain_steps: int = 10) -> dict:
+    """The 512-world sweep on one GPU: batched (graph replays, activity
+    readback every 60 substeps, wall clock) against the plain form (one
+    context per world, worlds stepped one after another on one stream, as
+    the reference's variant loop steps one SceneRunner at a time:
+    Apps/LifePresetLab/main.cpp:718-795)."""
+    import torch
+
+    import life_simulation_b200 as lb
+    from life_simulation_b200 import workloads as wl
+
+    specs, inits = wl.sweep512()
+    worlds = sweep_worlds(specs)
+    px = sum(w.width * w.height for w in worlds)
+    batched_s, activity, paths = sweep_batched(worlds, inits)
     mods = []
     for i, w in enumerate(worlds):
         conv = "fft" if paths[i] == lb.CONV_FFT else "direct"
@@ -878,8 +1016,6 @@ def run_sweep(args):
         m.reset(w.seed)
         m.upload(inits[i])
         mods.append(m)
-    # All contexts on one stream, so worlds run one after another as in the
-    # reference's variant loop (no overlap between worlds on the device).
     one = torch.cuda.Stream()
     sh = one.cuda_stream
     for m in mods:
@@ -895,14 +1031,59 @@ def run_sweep(args):
         m.close()
     batched = px * 240 / batched_s / 1e6
     plain = px * plain_steps / plain_s / 1e6
-    print(json.dumps({
-        "metric": "Lenia Mpixel-steps/s, 512-world sweep (batched vs one world at a time)",
-        "unit": UNIT, "value": batched, "plain": plain, "speedup": batched / plain,
-        "worlds": len(worlds), "pixels_per_step": px, "steps": 240,
-        "direct_worlds": paths.count(lb.CONV_DIRECT), "fft_worlds": paths.count(lb.CONV_FFT),
-        "activity": activity,
-        "timing": "wall clock incl. 4 activity readbacks (batched); plain: "
-                  f"{plain_steps} substeps per world, worlds in sequence"}))
+    return {"value": batched, "unit": UNIT, "plain": plain, "speedup": batched / plain,
+            "worlds": len(worlds), "pixels_per_step": px, "steps": 240,
+            "direct_worlds": paths.count(lb.CONV_DIRECT), "fft_worlds": paths.count(lb.CONV_FFT),
+            "activity": activity,
+            "timing": "wall clock incl. 4 activity readbacks (batched); plain: "
+                      f"{plain_steps} substeps per world, worlds in sequence on one stream"}
+
+
+def run_sweep(args):
+    """The 512-world sweep, batched against the plain form (one GPU), or
+    sharded by world over the ranks under torchrun."""
+    import torch
+
+    import life_simulation_b200 as lb
+    from life_simulation_b200 import workloads as wl
+    from life_simulation_b200.shard import loads, partition, world_cost
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world == 1:
+        line = {"metric": "Lenia Mpixel-steps/s, 512-world sweep (batched vs one world at a time)", "n_gpus": 1}
+        line.update(sweep_bench(args.plain_steps))
+        print(json.dumps(line))
+        return 0
+    import datetime
+
+    torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    specs, inits = wl.sweep512()
+    px_all = sum(s["width"] * s["height"] for s in specs)
+    # Each rank steps its cost-balanced share of the worlds as one batch;
+    # nothing crosses between GPUs until the final timing.
+    costs = [world_cost(s["width"], s["height"], s["radius"]) for s in specs]
+    shares = partition(costs, world)
+    mine = shares[rank]
+    torch.distributed.barrier()
+    batched_s, _, paths = sweep_batched(sweep_worlds([specs[i] for i in mine]), [inits[i] for i in mine])
+    t = torch.tensor([batched_s], device="cuda", dtype=torch.float64)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    batched_s = float(t.item())
+    n_direct = torch.tensor([paths.count(lb.CONV_DIRECT)], device="cuda")
+    torch.distributed.all_reduce(n_direct)
+    torch.cuda.synchronize()
+    torch.distributed.barrier()
+    torch.distributed.destroy_process_group()
+    if rank == 0:
+        print(json.dumps({
+            "metric": "Lenia Mpixel-steps/s, 512-world sweep (batched, worlds sharded over GPUs)",
+            "unit": UNIT, "value": px_all * 240 / batched_s / 1e6, "n_gpus": world, "scaling": "strong",
+            "worlds": 512, "pixels_per_step": px_all, "steps": 240, "direct_worlds": int(n_direct.item()),
+            "shares": [len(x) for x in shares],
+            "estimated_load_ratio": max(loads(costs, shares)) / min(loads(costs, shares)),
+            "timing": "wall clock incl. 4 activity readbacks, max over ranks; worlds assigned "
+                      "largest estimated cost first to the least-loaded rank"}))
     return 0
 
 

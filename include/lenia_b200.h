@@ -234,7 +234,8 @@ typedef struct lenia_profile_data {
 int lenia_profile(lenia_ctx* ctx, int enable);
 int lenia_profile_read(lenia_ctx* ctx, lenia_profile_data* out);
 /* Launch shapes of the spectral passes (extension; the reference has no
- * counterpart): columns per CTA of the column pass (8, 4 or 2) and rows per
+ * counterpart): columns per CTA of the column pass (8, 4, 2, or
+ * 4 | LENIA_COLS_HALF_THREADS) and rows per
  * CTA of the inverse row pass (4, 2 or 1, | LENIA_ROWS_PIPELINED for the
  * software-pipelined variant), as the setup autotuner picked them; 0, 0 on
  * the direct path and on the runtime-plan spectral path. lenia_set_tuning
@@ -242,6 +243,9 @@ int lenia_profile_read(lenia_ctx* ctx, lenia_profile_data* out);
  * made under the caller's own conditions); a shape the field size cannot
  * launch, or a context without these passes, is LENIA_ERR_INVALID_ARG. */
 #define LENIA_ROWS_PIPELINED 0x100
+/* Columns per CTA 4 | LENIA_COLS_HALF_THREADS: the column pass with half the
+ * threads per CTA, each thread taking two last-pass items. */
+#define LENIA_COLS_HALF_THREADS 0x40
 int lenia_get_tuning(lenia_ctx* ctx, int* cols_per_cta, int* rows_per_cta);
 int lenia_set_tuning(lenia_ctx* ctx, int cols_per_cta, int rows_per_cta);
 /* ---- Colour map (the module's output layer) ----

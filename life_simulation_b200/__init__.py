@@ -33,6 +33,7 @@ CONV_DIRECT, CONV_FFT, CONV_DIRECT_MULTI = 0, 1, 2
 CORE_GAUSS_SHELL, CORE_EXP = 0, 1
 FFT_FP32, FFT_BF16X3, FFT_FP16X3 = 0, 1, 2
 ROWS_PIPELINED = 0x100  # rows-per-CTA flag of the software-pipelined row pass
+COLS_HALF_THREADS = 0x40  # columns-per-CTA flag: half the threads, two last-pass items each
 INIT_NOISE, INIT_STAMP = 0, 1
 
 

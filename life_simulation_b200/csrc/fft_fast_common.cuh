@@ -91,8 +91,10 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 
 // Launch geometry of a column pass over B columns per CTA iteration (forward
 // plan PF; the inverse is PF reversed): T threads, ITL last-pass items per
-// thread, shared buffers of pitch PITCH.
-template <class PF, int B>
+// thread, shared buffers of pitch PITCH. S = 2 halves the thread count (each
+// thread takes two last-pass items): fewer warps per CTA, twice the
+// independent work per thread, and CTAs small enough for two per SM.
+template <class PF, int B, int S = 1>
 struct ColK {
     static_assert(KB % B == 0, "a column group lies inside one block");
     using PI = typename Reverse<PF>::type;
@@ -100,7 +102,7 @@ struct ColK {
     static constexpr int Hh = H / 2 + 1;
     static constexpr int RL = PF::last();
     static constexpr int NRL = H / RL;
-    static constexpr int T = roundup32(B * NRL);
+    static constexpr int T = roundup32((B * NRL + S - 1) / S);
     static constexpr int ITL = (B * NRL + T - 1) / T;
     static constexpr int PITCH = row_pitch(H);
     static constexpr size_t smem() {
@@ -109,15 +111,15 @@ struct ColK {
 };
 
 // Launch geometry of a row pass over RB rows per CTA iteration (inverse plan
-// PI; the forward is PI reversed).
-template <class PI, int RB>
+// PI; the forward is PI reversed); S as for ColK.
+template <class PI, int RB, int S = 1>
 struct RowK {
     using PF = typename Reverse<PI>::type;
     static constexpr int M = PI::n;
     static_assert(M % KB == 0, "row length must be a whole number of blocks");
     static constexpr int RC = PI::last();
     static constexpr int NRC = M / RC;
-    static constexpr int T = roundup32(RB * NRC);
+    static constexpr int T = roundup32((RB * NRC + S - 1) / S);
     static constexpr int ITL = (RB * NRC + T - 1) / T;
     static constexpr int PITCH = row_pitch(M);  // even: rows start 16-byte aligned
     // Twiddle tables, then the buffers from an even float2 offset so the

@@ -939,7 +939,7 @@ cudaError_t autotune(lenia_adjoint* a) {
         return r;
     };
     float best = 1e30f;
-    for (int cb : {8, 4, 2}) {
+    for (int cb : lenia::kColCandidates) {
         float ms = 0.0f;
         const cudaError_t r = timed([&] {
             return lenia::launch_col_fast_worlds(a->H, a->M, a->ft, cb, a->d_fcol, a->nb, s);

@@ -584,7 +584,7 @@ int lenia_batch_create(const lenia_world* worlds, uint32_t n, uint32_t policy, l
             for (auto& c : b.classes) {
                 const int cnt = int(c.ids.size());
                 float best = 1e30f;
-                for (int cb : {8, 4, 2}) {
+                for (int cb : kColCandidates) {
                     const float ms = time_ms([&] { return launch_col_fast_worlds(c.H, c.M, c.t, cb, c.d_stab[0], cnt, b.stream); });
                     if (ms < 0.97f * best) { best = ms; c.col_batch = cb; }
                 }

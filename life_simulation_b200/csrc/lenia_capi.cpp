@@ -354,6 +354,7 @@ int lenia_profile_read(lenia_ctx* c, lenia_profile_data* out) {
 }
 
 static_assert(LENIA_ROWS_PIPELINED == lenia::kRowPipelined, "pipelined row flag");
+static_assert(LENIA_COLS_HALF_THREADS == lenia::kHalfThreads, "half-thread column flag");
 
 int lenia_get_tuning(lenia_ctx* c, int* cols, int* rows) {
     if (!c || !cols || !rows) return LENIA_ERR_INVALID_ARG;

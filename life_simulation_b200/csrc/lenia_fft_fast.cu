@@ -55,21 +55,22 @@ using namespace fastfft;
 // Shared-memory staging of the next column group's row spectrum (B columns
 // x H rows, row-major, 16-byte asynchronous copies): used when B is even and
 // the extra buffer fits the 227 KB a CTA may have.
-template <class PF, int B>
+template <class PF, int B, int S = 1>
 struct ColStage {
-    using K = ColK<PF, B>;
+    using K = ColK<PF, B, S>;
     static constexpr int OFF =
         (PF::tw_size() + K::PI::tw_size() + 2 * B * K::PITCH + K::H + 1) / 2 * 2;  // 16-byte aligned
     static constexpr size_t with_stage = sizeof(float2) * (size_t(OFF) + size_t(B) * K::H);
-    static constexpr bool on = B % 2 == 0 && with_stage <= 227 * 1024;
+    // Not with S = 2, whose CTAs are meant to fit two per SM.
+    static constexpr bool on = S == 1 && B % 2 == 0 && with_stage <= 227 * 1024;
     static constexpr size_t smem() { return on ? with_stage : K::smem(); }
 };
 
-template <class PF, int B>
-__global__ void __launch_bounds__(ColK<PF, B>::T)
+template <class PF, int B, int SPLIT>
+__global__ void __launch_bounds__(ColK<PF, B, SPLIT>::T)
     col_fast_kernel(SpectralWorld w0, const SpectralWorld* __restrict__ worlds,
                     const float2* __restrict__ twf_g, const float2* __restrict__ twi_g) {
-    using K = ColK<PF, B>;
+    using K = ColK<PF, B, SPLIT>;
     using PI = typename K::PI;
     using IL = PassIdx<PF, PF::np - 1>;
     constexpr int H = K::H, T = K::T, PITCH = K::PITCH, RL = K::RL, NRL = K::NRL, Hh = K::Hh;
@@ -89,7 +90,7 @@ __global__ void __launch_bounds__(ColK<PF, B>::T)
     float2* __restrict__ U = sw.U;
     const float* __restrict__ khat = sw.khat;
     const int M = sw.M, nk = sw.nk;
-    using CS = ColStage<PF, B>;
+    using CS = ColStage<PF, B, SPLIT>;
     float2* bs = sm + CS::OFF;
     // Rows of columns g0..g0+B-1 of S into bs as bs[i * B + b].
     const auto stage_group = [&](int g0) {
@@ -247,12 +248,13 @@ static __device__ __noinline__ void palette_pair(const ColorMapParams& cm, float
 // (one staging buffer, which doubles as the second work buffer) each item is
 // staged and waited for in turn: less shared memory per CTA, which wins
 // where shared memory limits the resident CTAs (long rows).
-template <class PI, int RB, bool PIPE, bool CM>
-__global__ void __launch_bounds__(RowK<PI, RB>::T, (512 / RowK<PI, RB>::T > 1 ? 512 / RowK<PI, RB>::T : 1))
+template <class PI, int RB, bool PIPE, bool CM, int SPLIT>
+__global__ void __launch_bounds__(RowK<PI, RB, SPLIT>::T,
+                                  (512 / RowK<PI, RB, SPLIT>::T > 1 ? 512 / RowK<PI, RB, SPLIT>::T : 1))
     row_fast_kernel(SpectralWorld w0, const SpectralWorld* __restrict__ worlds,
                     const float2* __restrict__ twr_g, const float2* __restrict__ twi_g,
                     const float2* __restrict__ twf_g) {
-    using K = RowK<PI, RB>;
+    using K = RowK<PI, RB, SPLIT>;
     using PF = typename K::PF;
     using IL = PassIdx<PI, PI::np - 1>;
     constexpr int M = K::M, W = 2 * M, T = K::T, PITCH = K::PITCH, RC = K::RC, NRC = K::NRC;
@@ -438,12 +440,12 @@ void plan_radices(FastPlan& out) {
     for (int i = 0; i < P::np; ++i) out.radix[i] = P::radix(i);
 }
 
-template <class PF, int B>
+template <class PF, int B, int S = 1>
 cudaError_t launch_col_t(const SpectralWorld& w0, const SpectralWorld* worlds, int n, int M,
                          const FastTables& t, cudaStream_t s) {
-    using K = ColK<PF, B>;
-    auto fn = col_fast_kernel<PF, B>;
-    const size_t smem = ColStage<PF, B>::smem();
+    using K = ColK<PF, B, S>;
+    auto fn = col_fast_kernel<PF, B, S>;
+    const size_t smem = ColStage<PF, B, S>::smem();
     if (smem > 227 * 1024 || K::T > 1024) return cudaErrorInvalidConfiguration;
     cudaError_t e = prepare(fn, smem);
     if (e != cudaSuccess) return e;
@@ -452,11 +454,11 @@ cudaError_t launch_col_t(const SpectralWorld& w0, const SpectralWorld* worlds, i
     return launch_chained(fn, world_grid(per, (M + B - 1) / B, n), K::T, smem, s, w0, worlds, t.col_twf, t.col_twi);
 }
 
-template <class PI, int RB, bool PIPE, bool CM>
+template <class PI, int RB, bool PIPE, bool CM, int S = 1>
 cudaError_t launch_row_t(const SpectralWorld& w0, const SpectralWorld* worlds, int n, int H,
                          const float2* tw_r2c, const FastTables& t, cudaStream_t s) {
-    using K = RowK<PI, RB>;
-    auto fn = row_fast_kernel<PI, RB, PIPE, CM>;
+    using K = RowK<PI, RB, S>;
+    auto fn = row_fast_kernel<PI, RB, PIPE, CM, S>;
     const size_t smem = K::smem(PIPE ? 3 : 2);
     if (smem > 227 * 1024) return cudaErrorInvalidConfiguration;
     cudaError_t e = prepare(fn, smem);
@@ -524,10 +526,11 @@ namespace {
 cudaError_t col_dispatch(int H, int M, int batch, const SpectralWorld& w0, const SpectralWorld* worlds, int n,
                          const FastTables& t, cudaStream_t s) {
     switch (H) {
-#define X(h, ...)                                                                       \
-    case h:                                                                             \
-        if (batch == 8) return launch_col_t<__VA_ARGS__, 8>(w0, worlds, n, M, t, s);    \
-        if (batch == 4) return launch_col_t<__VA_ARGS__, 4>(w0, worlds, n, M, t, s);    \
+#define X(h, ...)                                                                                  \
+    case h:                                                                                        \
+        if (batch == (4 | kHalfThreads)) return launch_col_t<__VA_ARGS__, 4, 2>(w0, worlds, n, M, t, s); \
+        if (batch == 8) return launch_col_t<__VA_ARGS__, 8>(w0, worlds, n, M, t, s);               \
+        if (batch == 4) return launch_col_t<__VA_ARGS__, 4>(w0, worlds, n, M, t, s);               \
         return launch_col_t<__VA_ARGS__, 2>(w0, worlds, n, M, t, s);
         LENIA_COL_PLANS(X)
 #undef X
@@ -541,8 +544,9 @@ cudaError_t col_dispatch(int H, int M, int batch, const SpectralWorld& w0, const
 template <bool CM>
 cudaError_t row_dispatch_t(int H, int M, int batch, const SpectralWorld& w0, const SpectralWorld* worlds, int n,
                            const float2* tw_r2c, const FastTables& t, cudaStream_t s) {
-    const int rb = batch & ~kRowPipelined;
+    const int rb = batch & 7;
     const bool pipe = (batch & kRowPipelined) != 0;
+    if (batch & kHalfThreads) return cudaErrorInvalidConfiguration;  // columns only
     switch (M) {
 #define X(m, ...)                                                                                      \
     case m:                                                                                            \
@@ -566,15 +570,15 @@ cudaError_t row_dispatch(int H, int M, int batch, const SpectralWorld& w0, const
     return row_dispatch_t<false>(H, M, batch, w0, worlds, n, tw_r2c, t, s);
 }
 
-template <class PF, int B>
+template <class PF, int B, int S = 1>
 bool col_shape_ok() {
-    using K = ColK<PF, B>;
-    return K::T <= 1024 && ColStage<PF, B>::smem() <= 227 * 1024;
+    using K = ColK<PF, B, S>;
+    return K::T <= 1024 && ColStage<PF, B, S>::smem() <= 227 * 1024;
 }
 
-template <class PI, int RB, bool PIPE>
+template <class PI, int RB, bool PIPE, int S = 1>
 bool row_shape_ok() {
-    using K = RowK<PI, RB>;
+    using K = RowK<PI, RB, S>;
     return K::T <= 1024 && K::smem(PIPE ? 3 : 2) <= 227 * 1024;
 }
 
@@ -585,15 +589,16 @@ bool fast_shapes_supported(int H, int M, int col_batch, int row_batch) {
     switch (H) {
 #define X(h, ...)                                                        \
     case h:                                                              \
-        col = col_batch == 8   ? col_shape_ok<__VA_ARGS__, 8>()          \
-              : col_batch == 4 ? col_shape_ok<__VA_ARGS__, 4>()          \
-              : col_batch == 2 ? col_shape_ok<__VA_ARGS__, 2>() : false; \
+        col = col_batch == 8                    ? col_shape_ok<__VA_ARGS__, 8>()    \
+              : col_batch == 4                  ? col_shape_ok<__VA_ARGS__, 4>()    \
+              : col_batch == (4 | kHalfThreads) ? col_shape_ok<__VA_ARGS__, 4, 2>() \
+              : col_batch == 2                  ? col_shape_ok<__VA_ARGS__, 2>() : false; \
         break;
         LENIA_COL_PLANS(X)
 #undef X
     default: break;
     }
-    const int rb = row_batch & ~kRowPipelined;
+    const int rb = row_batch & 7;
     const bool pipe = (row_batch & kRowPipelined) != 0;
     if ((row_batch & ~(kRowPipelined | 7)) != 0) return false;
     switch (M) {

@@ -155,7 +155,12 @@ bool fast_twiddle_tables(int H, int M, std::vector<float2> (&out)[4]);
 // row spectrum of A into S_next (U, A_out unused). The row pass stages A with
 // 16-byte copies: A must be 16-byte aligned.
 constexpr int kRowPipelined = 0x100;
-// The row-batch candidates an autotuner times.
+// Columns per CTA | kHalfThreads (4 only): the column pass with half the
+// threads per CTA, each taking two last-pass items (twice the independent
+// work per thread).
+constexpr int kHalfThreads = 0x40;
+// The candidates an autotuner times.
+constexpr int kColCandidates[4] = {8, 4, 2, 4 | kHalfThreads};
 constexpr int kRowCandidates[6] = {4, 2, 1, 4 | kRowPipelined, 2 | kRowPipelined, 1 | kRowPipelined};
 // Whether columns per CTA `col_batch` (8/4/2) and rows per CTA `row_batch`
 // (4/2/1, optionally | kRowPipelined) launch for an H x 2M field on the

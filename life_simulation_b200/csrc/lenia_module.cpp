@@ -1005,14 +1005,18 @@ int LeniaModule::autotuneSpectral() {
     const char* log_env = std::getenv("LENIA_AUTOTUNE_LOG");
     const bool log = log_env && *log_env && *log_env != '0';
     float best_col = 1e30f, best_row = 1e30f;
-    for (int c : {8, 4, 2}) {
+    for (int c : kColCandidates) {
+        if (!fast_shapes_supported(int(h_), int(w_ / 2), c, 4)) continue;
         const float t = time_it([&] { return launch_col_fast(fgeo_, fast_, c, d_S_, d_U_, stream_); });
-        if (log) std::fprintf(stderr, "lenia autotune %ux%u column cols/CTA %d: %.4f ms\n", w_, h_, c, t);
+        if (log)
+            std::fprintf(stderr, "lenia autotune %ux%u column cols/CTA %d%s: %.4f ms\n", w_, h_, c & 0xF,
+                         (c & kHalfThreads) ? " half threads" : "", t);
         if (t < 0.97f * best_col) { best_col = t; col_batch_ = c; }
     }
     // Row candidates are timed as they run in a step: three column + row
     // pairs back to back (the row pass follows the column pass it reads).
     for (int c : kRowCandidates) {
+        if (!fast_shapes_supported(int(h_), int(w_ / 2), col_batch_, c)) continue;
         const float t = time_it([&] {
             cudaError_t e = cudaSuccess;
             for (int i = 0; i < 3 && e == cudaSuccess; ++i) {
@@ -1023,7 +1027,7 @@ int LeniaModule::autotuneSpectral() {
             return e;
         });
         if (log)
-            std::fprintf(stderr, "lenia autotune %ux%u 3 steps with rows/CTA %d%s: %.4f ms\n", w_, h_, c & ~kRowPipelined,
+            std::fprintf(stderr, "lenia autotune %ux%u 3 steps with rows/CTA %d%s: %.4f ms\n", w_, h_, c & 7,
                          (c & kRowPipelined) ? " pipelined" : "", t);
         if (t < 0.97f * best_row) { best_row = t; row_batch_ = c; }
     }

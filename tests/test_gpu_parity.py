@@ -228,9 +228,10 @@ def test_every_launch_shape_gives_the_same_bits(w, h):
     init = wl.patches(w, h, 8, 64, seed=6)
     m = lb.LeniaModule(p, w, h)
     cols, rows = m.tuning()
-    assert cols in (8, 4, 2) and rows & ~lb.ROWS_PIPELINED in (4, 2, 1)
+    assert cols in (8, 4, 2, 4 | lb.COLS_HALF_THREADS) and rows & ~lb.ROWS_PIPELINED in (4, 2, 1)
     ref = None
-    shapes = [(c, r | f) for c in (8, 4, 2) for r in (4, 2, 1) for f in (0, lb.ROWS_PIPELINED)]
+    shapes = [(c, r | f) for c in (8, 4, 2, 4 | lb.COLS_HALF_THREADS) for r in (4, 2, 1)
+              for f in (0, lb.ROWS_PIPELINED)]
     ran = 0
     for c, r in shapes:
         try:
@@ -248,7 +249,8 @@ def test_every_launch_shape_gives_the_same_bits(w, h):
         np.testing.assert_array_equal(out, ref, err_msg=f"{c} columns, {r:#x} rows per CTA")
         ran += 1
     assert ran >= 6
-    for bad in ((3, 2), (4, 3), (4, 8), (16, 1), (4, 2 | 0x200)):
+    for bad in ((3, 2), (4, 3), (4, 8), (16, 1), (4, 2 | 0x200), (8 | lb.COLS_HALF_THREADS, 2),
+                (4, 2 | lb.COLS_HALF_THREADS)):
         with pytest.raises(lb.LeniaError, match="unsupported launch shape"):
             m.set_tuning(*bad)
     m.close()
