@@ -226,6 +226,21 @@ def cpu_baseline_port(params, w, h, init, seconds):
             "sample": f"full {w}x{h} field, {steps} substeps in {el:.1f} s (FP64 oracle)"}
 
 
+_FP32_PEAK = None
+
+
+def fp32_peak_measured() -> dict:
+    """The device's FP32 FMA peak measured by lenia_fp32_peak (scalar FFMA,
+    the instruction the direct kernel issues; packed FFMA2 beside it)."""
+    global _FP32_PEAK
+    if _FP32_PEAK is None:
+        import life_simulation_b200 as lb
+        r = lb.fp32_peak(5)
+        r["source"] = "measured (lenia_fp32_peak: 8 FMA chains per thread, 8 x 256 threads per SM)"
+        _FP32_PEAK = r
+    return _FP32_PEAK
+
+
 def published_direct_bench(steps: int = 50, warmup: int = 5) -> dict:
     """The reference's published direct configuration: one kernel, R=32,
     1280x720 (README.md:47-48, 19.4 ms per frame on an Apple M5 Max, one
@@ -259,9 +274,18 @@ def published_direct_bench(steps: int = 50, warmup: int = 5) -> dict:
     info = m.info()
     m.close()
     ref_ms = 19.4
+    # FP32 roofline: 2 FLOP per nonzero tap + 12 for the growth map, per pixel.
+    flops = (2 * info["direct_taps"] + 12) * w * h
+    peak = fp32_peak_measured()
+    tflops = flops / (ms / 1e3) / 1e12
     return {"workload": "direct, 1 kernel R=32, 1280x720 (the reference's published direct configuration)",
             "ms_per_step": ms, "value": w * h / (ms / 1e3) / 1e6, "unit": UNIT,
             "direct_tma": info["direct_tma"], "direct_split": info["direct_split"],
+            "direct_outputs_per_thread": info["direct_outputs_per_thread"],
+            "direct_rows_per_thread": info["direct_rows_per_thread"],
+            "fp32": {"achieved_tflops": tflops, "peak_tflops": peak["ffma_tflops"],
+                     "frac": tflops / peak["ffma_tflops"], "peak_source": peak["source"],
+                     "algorithmic_flops_per_step": flops},
             "reference_published": {"ms_per_frame": ref_ms, "value": w * h / (ref_ms / 1e3) / 1e6,
                                     "hardware": "Apple M5 Max (Metal), README.md:47-48; not reproducible here"}}
 
@@ -719,10 +743,11 @@ def run_b200(args):
                                           "rows_pipelined": bool(shape[1] & lb.ROWS_PIPELINED),
                                           "chosen_by": chosen_by}
     if direct_flops is not None:
-        fp32_peak = 148 * 128 * 2 * 1.965e9 / 1e12  # nominal FP32 FMA TFLOP/s (no measured figure)
+        pk = fp32_peak_measured()
+        fp32_peak = pk["ffma_tflops"]
         tflops = direct_flops / (launch_ms / 1e3) / 1e12
         roofline = {"bound": "fp32", "kernel": dom, "achieved": tflops, "peak": fp32_peak,
-                    "peak_source": "nominal (148 SMs x 128 FP32 lanes x 2 x 1.965 GHz)", "unit": "TFLOP/s",
+                    "peak_source": pk["source"], "unit": "TFLOP/s",
                     "frac": tflops / fp32_peak, "traffic": None, "algorithmic_flops_per_launch": direct_flops,
                     "launch_ms": launch_ms}
     else:
@@ -756,6 +781,8 @@ def run_b200(args):
     if rank == 0 and world == 1 and args.workload == WORKLOAD:
         line["published_config"] = published_config_bench()
         line["published_direct_config"] = published_direct_bench()
+    if rank == 0 and world == 1:
+        line["fp32_peak"] = fp32_peak_measured()
     if rank == 0 and world == 1 and not args.no_sweep:
         line["sweep"] = sweep_bench(args.plain_steps)
     if rank == 0 and world == 1 and not args.no_tc:

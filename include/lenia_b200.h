@@ -131,6 +131,7 @@ typedef struct lenia_info {
     uint32_t direct_split;    /* direct path: thread groups sharing a tile's kernel rows (1, 2, 4, 8) */
     uint32_t direct_outputs_per_thread; /* direct path: 8, or 16 on large tiles where faster */
     uint32_t direct_taps;     /* direct path: nonzero kernel taps summed over its kernels */
+    uint32_t direct_rows_per_thread; /* direct path: output rows per thread, 1 or 2 (large tiles where faster) */
 } lenia_info;
 
 typedef struct lenia_ctx lenia_ctx;
@@ -511,6 +512,14 @@ int lenia_create_scene_module(const char* scene_json, const char* module_name, l
 /* Reads per-frame parameters from `bus` from now on (NULL: the context's own
  * bus again). The bus must outlive the attachment. */
 int lenia_attach_bus(lenia_ctx* ctx, lenia_bus* bus);
+
+/* ---- Device characterisation ----
+ * The FP32 fused multiply-add peak of the current device, measured: 8
+ * independent FMA chains per thread, 8 CTAs of 256 threads per SM, best of
+ * `reps` timed launches (CUDA events on `stream`) of a scalar-FFMA kernel and
+ * of a packed-FFMA2 kernel, in TFLOP/s (2 FLOP per FMA). The denominator of
+ * the direct path's FLOP/s roofline. No counterpart in the reference. */
+int lenia_fp32_peak(int reps, double* tflops_ffma, double* tflops_ffma2, void* stream);
 
 /* Message of the last warning or error on this context ("" if none). */
 const char* lenia_last_message(lenia_ctx* ctx);

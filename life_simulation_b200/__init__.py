@@ -83,7 +83,8 @@ class Info(ctypes.Structure):
                 ("device_bytes", ctypes.c_uint64), ("fft_radix_row", ctypes.c_uint32 * 8),
                 ("fft_radix_col", ctypes.c_uint32 * 8), ("fft_precision", ctypes.c_uint32),
                 ("direct_tma", ctypes.c_uint32), ("direct_split", ctypes.c_uint32),
-                ("direct_outputs_per_thread", ctypes.c_uint32), ("direct_taps", ctypes.c_uint32)]
+                ("direct_outputs_per_thread", ctypes.c_uint32), ("direct_taps", ctypes.c_uint32),
+                ("direct_rows_per_thread", ctypes.c_uint32)]
 
 
 # Every symbol include/lenia_b200.h declares (checked by the CPU tests).
@@ -96,7 +97,7 @@ EXPORTS = (
     "lenia_download_device", "lenia_field_device_ptr", "lenia_get_info",
     "lenia_get_stream", "lenia_profile", "lenia_profile_read", "lenia_get_tuning", "lenia_set_tuning",
     "lenia_last_message", "lenia_status_string",
-    "lenia_fft_step_noalloc", "lenia_noalloc_last_message",
+    "lenia_fft_step_noalloc", "lenia_noalloc_last_message", "lenia_fp32_peak",
     "lenia_batch_create", "lenia_batch_destroy", "lenia_batch_upload", "lenia_batch_download",
     "lenia_batch_step", "lenia_batch_stats", "lenia_batch_world_path", "lenia_batch_sync",
     "lenia_batch_last_message",
@@ -214,6 +215,7 @@ def load_library(path: str = LIB_PATH):
                                          ctypes.POINTER(FrameParams), u32, P]
     L.lenia_noalloc_last_message.argtypes = []
     L.lenia_noalloc_last_message.restype = ctypes.c_char_p
+    L.lenia_fp32_peak.argtypes = [i32, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double), P]
     L.lenia_batch_create.argtypes = [ctypes.POINTER(World), u32, u32, pp]
     L.lenia_batch_destroy.argtypes = [P]
     L.lenia_batch_upload.argtypes = [P, u32, P]
@@ -495,7 +497,8 @@ class LeniaModule:
                 "fft_radix_row": [r for r in i.fft_radix_row if r],
                 "fft_radix_col": [r for r in i.fft_radix_col if r], "fft_precision": i.fft_precision,
                 "direct_tma": bool(i.direct_tma), "direct_split": i.direct_split,
-                "direct_outputs_per_thread": i.direct_outputs_per_thread, "direct_taps": i.direct_taps}
+                "direct_outputs_per_thread": i.direct_outputs_per_thread, "direct_taps": i.direct_taps,
+                "direct_rows_per_thread": i.direct_rows_per_thread}
 
 
 def inspect(params, scene_w: int, scene_h: int, base_dir: Optional[str] = None) -> dict:
@@ -515,6 +518,17 @@ def inspect(params, scene_w: int, scene_h: int, base_dir: Optional[str] = None) 
             "fft_radix_row": [r for r in i.fft_radix_row if r],
             "fft_radix_col": [r for r in i.fft_radix_col if r],
             "status": rc, "warning": msg if rc > 0 else ""}
+
+
+def fp32_peak(reps: int = 5, stream: Optional[int] = None) -> dict:
+    """Measured FP32 FMA peak of the current device in TFLOP/s: scalar FFMA
+    and packed FFMA2 (lenia_fp32_peak)."""
+    L = load_library()
+    a, b = ctypes.c_double(), ctypes.c_double()
+    rc = L.lenia_fp32_peak(reps, ctypes.byref(a), ctypes.byref(b), ctypes.c_void_p(stream) if stream else None)
+    if rc != 0:
+        raise LeniaError(rc, "lenia_fp32_peak failed")
+    return {"ffma_tflops": a.value, "ffma2_tflops": b.value}
 
 
 def make_frame_params(dt=0.1, growth_mu=0.15, growth_sigma=0.017, noise_amount=0.0, mu_jitter=0.0,

@@ -36,11 +36,13 @@ namespace {
 constexpr int PX = 8;  // taps per chunk along x (and the default outputs per thread)
 
 // OX outputs per thread along x: 8, or 16 on large tiles (half the input
-// loads per multiply-add; each output's sum runs in the same order either
-// way, so the two give the same bits).
-template <int TW, int TH, int OX = PX>
+// loads per multiply-add); OY output rows per thread: 1, or 2 on large tiles
+// (each staged input row chunk then feeds two kernel rows: half the input
+// loads again). Each output's sum runs in the same order in every variant,
+// so they all give the same bits.
+template <int TW, int TH, int OX = PX, int OY = 1>
 struct DirectTile {
-    static constexpr int kThreads = (TW / OX) * TH;
+    static constexpr int kThreads = (TW / OX) * (TH / OY);
 };
 
 // Per-kernel-row chunk plan, filled on the host: for row dy (0..2R), the first
@@ -94,7 +96,7 @@ constexpr uint32_t kTmaPolls = 1u << 22;
 // s + S, ...) for fields too small to fill the GPU one thread per 8 outputs:
 // the groups' partial sums meet in shared memory and are added in group
 // order before the epilogue.
-template <int TW, int TH, int NK, int S = 1, int OX = PX>
+template <int TW, int TH, int NK, int S = 1, int OX = PX, int OY = 1>
 __device__ __forceinline__ void direct_tile(const float* __restrict__ src, float* __restrict__ dst,
                                             const float* __restrict__ weights,  // [NK][2R+1][WP], zero padded
                                             const uint32_t* __restrict__ spans, // [NK][2R+1]
@@ -110,7 +112,8 @@ __device__ __forceinline__ void direct_tile(const float* __restrict__ src, float
 
     const int W = int(p.width), H = int(p.height);
     const int tid = threadIdx.x;
-    constexpr int NT0 = DirectTile<TW, TH, OX>::kThreads;  // threads per row group
+    static_assert(OY == 1 || S == 1, "two output rows per thread only without the kernel-row split");
+    constexpr int NT0 = DirectTile<TW, TH, OX, OY>::kThreads;  // threads per row group
     constexpr int NT = NT0 * S;
     const int grp = S > 1 ? tid / NT0 : 0;
     const int lt = tid - grp * NT0;
@@ -160,14 +163,67 @@ __device__ __forceinline__ void direct_tile(const float* __restrict__ src, float
     }
     __syncthreads();
 
-    const int tx = lt % (TW / OX), ty = lt / (TW / OX);
+    const int tx = lt % (TW / OX), ty = lt / (TW / OX) * OY;  // ty: first output row within the tile
     const int ox = tx * OX;  // first output column within the tile
-    float acc[NK][OX];
+    float acc[OY][NK][OX];
 #pragma unroll
-    for (int k = 0; k < NK; ++k)
+    for (int o = 0; o < OY; ++o)
 #pragma unroll
-        for (int j = 0; j < OX; ++j) acc[k][j] = 0.0f;
+        for (int k = 0; k < NK; ++k)
+#pragma unroll
+            for (int j = 0; j < OX; ++j) acc[o][k][j] = 0.0f;
 
+    if constexpr (OY > 1) {
+        // Walk the input rows ty + r; row r meets kernel row dy = r - o of
+        // output row ty + o. A chunk of the row is loaded once for every
+        // kernel row it meets: the union of those rows' chunk spans (spans
+        // lie on one 8-tap grid, and taps outside a row's own span weigh
+        // zero, adding an exact +0 to its sums). Each output still sums its
+        // kernel rows in ascending dy and taps in ascending dx.
+#pragma unroll
+        for (int k = 0; k < NK; ++k) {
+            for (int r = 0; r < g.ksize + OY - 1; ++r) {
+                int lo = 1 << 20, hi = -(1 << 20);
+#pragma unroll
+                for (int o = 0; o < OY; ++o) {
+                    const int dyi = r - o;
+                    if (dyi < 0 || dyi >= g.ksize) continue;
+                    int start, count;
+                    unpack_span(sp[k * g.ksize + dyi], start, count);
+                    if (count > 0) {
+                        lo = min(lo, start);
+                        hi = max(hi, start + count * PX);
+                    }
+                }
+                const float* in_row = tile + (ty + r) * TP + ox + g.xp;
+                for (int d0 = lo; d0 < hi; d0 += PX) {
+                    const float4* ip = reinterpret_cast<const float4*>(in_row + d0);
+                    float in[OX + PX];
+#pragma unroll
+                    for (int q = 0; q < (OX + PX) / 4; ++q) {
+                        const float4 a = ip[q];
+                        in[4 * q] = a.x;
+                        in[4 * q + 1] = a.y;
+                        in[4 * q + 2] = a.z;
+                        in[4 * q + 3] = a.w;
+                    }
+#pragma unroll
+                    for (int o = 0; o < OY; ++o) {
+                        const int dyi = r - o;
+                        if (dyi < 0 || dyi >= g.ksize) continue;
+                        const float4* wp =
+                            reinterpret_cast<const float4*>(wts + (k * g.ksize + dyi) * g.wp + g.xp + d0);
+                        const float4 w0 = wp[0], w1 = wp[1];
+                        const float wv[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
+#pragma unroll
+                        for (int i = 0; i < PX; ++i)
+#pragma unroll
+                            for (int j = 0; j < OX; ++j) acc[o][k][j] = fmaf(wv[i], in[i + j], acc[o][k][j]);
+                    }
+                }
+            }
+        }
+    } else {
 #pragma unroll
     for (int k = 0; k < NK; ++k) {
         for (int dyi = grp; dyi < g.ksize; dyi += S) {
@@ -194,9 +250,10 @@ __device__ __forceinline__ void direct_tile(const float* __restrict__ src, float
 #pragma unroll
                 for (int i = 0; i < PX; ++i)
 #pragma unroll
-                    for (int j = 0; j < OX; ++j) acc[k][j] = fmaf(wv[i], in[i + j], acc[k][j]);
+                    for (int j = 0; j < OX; ++j) acc[0][k][j] = fmaf(wv[i], in[i + j], acc[0][k][j]);
             }
         }
+    }
     }
 
     if constexpr (S > 1) {
@@ -205,7 +262,7 @@ __device__ __forceinline__ void direct_tile(const float* __restrict__ src, float
 #pragma unroll
             for (int k = 0; k < NK; ++k)
 #pragma unroll
-                for (int j = 0; j < OX; ++j) part[(((grp - 1) * NK + k) * NT0 + lt) * OX + j] = acc[k][j];
+                for (int j = 0; j < OX; ++j) part[(((grp - 1) * NK + k) * NT0 + lt) * OX + j] = acc[0][k][j];
         }
         __syncthreads();
         if (grp > 0) return;
@@ -213,32 +270,35 @@ __device__ __forceinline__ void direct_tile(const float* __restrict__ src, float
 #pragma unroll
             for (int k = 0; k < NK; ++k)
 #pragma unroll
-                for (int j = 0; j < OX; ++j) acc[k][j] += part[(((q - 1) * NK + k) * NT0 + lt) * OX + j];
+                for (int j = 0; j < OX; ++j) acc[0][k][j] += part[(((q - 1) * NK + k) * NT0 + lt) * OX + j];
     }
-    const int gy = y0 + ty;
-    if (gy >= H) return;
-    const float* arow = tile + (ty + g.r) * TP + ox + g.xp;
 #pragma unroll
-    for (int j = 0; j < OX; ++j) {
-        const int gx = x0 + ox + j;
-        if (gx >= W) break;
-        const float A = arow[j];
-        const float muJ = mu_jitter_shift(p, uint32_t(gx), uint32_t(gy));
-        GrowthAcc ga;
+    for (int o = 0; o < OY; ++o) {
+        const int gy = y0 + ty + o;
+        if (gy >= H) return;
+        const float* arow = tile + (ty + o + g.r) * TP + ox + g.xp;
 #pragma unroll
-        for (int k = 0; k < NK; ++k) ga.add(p.weight[k], bell(acc[k][j], p.mu[k] + muJ, p.sigma[k]));
-        dst[size_t(gy) * W + gx] = growth_finish(p, A, ga, uint32_t(gx), uint32_t(gy));
+        for (int j = 0; j < OX; ++j) {
+            const int gx = x0 + ox + j;
+            if (gx >= W) break;
+            const float A = arow[j];
+            const float muJ = mu_jitter_shift(p, uint32_t(gx), uint32_t(gy));
+            GrowthAcc ga;
+#pragma unroll
+            for (int k = 0; k < NK; ++k) ga.add(p.weight[k], bell(acc[o][k][j], p.mu[k] + muJ, p.sigma[k]));
+            dst[size_t(gy) * W + gx] = growth_finish(p, A, ga, uint32_t(gx), uint32_t(gy));
+        }
     }
 }
 
-template <int TW, int TH, int NK, int S, int OX>
-__global__ void __launch_bounds__(DirectTile<TW, TH, OX>::kThreads * S)
+template <int TW, int TH, int NK, int S, int OX, int OY>
+__global__ void __launch_bounds__(DirectTile<TW, TH, OX, OY>::kThreads * S)
     direct_step_kernel(const float* __restrict__ src, float* __restrict__ dst,
                        const float* __restrict__ weights, const uint32_t* __restrict__ spans,
                        DirectGeometry g, StepParams p, const __grid_constant__ CUtensorMap tmap, int use_tma,
                        int* err) {
-    direct_tile<TW, TH, NK, S, OX>(src, dst, weights, spans, g, p, blockIdx.x * TW, blockIdx.y * TH,
-                                   use_tma ? &tmap : nullptr, err);
+    direct_tile<TW, TH, NK, S, OX, OY>(src, dst, weights, spans, g, p, blockIdx.x * TW, blockIdx.y * TH,
+                                       use_tma ? &tmap : nullptr, err);
 }
 
 // Many worlds in one launch: CTA i computes tile tiles[i] = (world, tile x,
@@ -254,15 +314,15 @@ __global__ void __launch_bounds__(DirectTile<TW, TH>::kThreads)
     direct_tile<TW, TH, 1>(w.src, w.dst, w.weights, w.spans, w.g, w.p, t.y * TW, t.z * TH, nullptr, nullptr);
 }
 
-template <int TW, int TH, int NK, int S, int OX>
+template <int TW, int TH, int NK, int S, int OX, int OY>
 cudaError_t launch_t(const float* src, float* dst, const float* weights, const uint32_t* spans,
                      const DirectGeometry& g, const StepParams& p, cudaStream_t stream, const DirectTma* tma,
                      int buffer) {
     const int TP = TW + 2 * g.xp + 8;
     const size_t smem = sizeof(float) * (size_t(TH + 2 * g.r) * TP + size_t(NK) * g.ksize * g.wp) +
                         sizeof(uint32_t) * NK * g.ksize +
-                        sizeof(float) * size_t(S - 1) * NK * DirectTile<TW, TH, OX>::kThreads * OX;
-    auto fn = direct_step_kernel<TW, TH, NK, S, OX>;
+                        sizeof(float) * size_t(S - 1) * NK * DirectTile<TW, TH, OX, OY>::kThreads * OX;
+    auto fn = direct_step_kernel<TW, TH, NK, S, OX, OY>;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;
     CUtensorMap map;
@@ -270,20 +330,20 @@ cudaError_t launch_t(const float* src, float* dst, const float* weights, const u
     const bool on = tma && tma->on && (buffer == 0 || buffer == 1);
     if (on) std::memcpy(&map, tma->map[buffer], sizeof map);
     dim3 grid((p.width + TW - 1) / TW, (p.height + TH - 1) / TH);
-    fn<<<grid, DirectTile<TW, TH, OX>::kThreads * S, smem, stream>>>(src, dst, weights, spans, g, p, map, on ? 1 : 0,
-                                                                 on ? tma->err : nullptr);
+    fn<<<grid, DirectTile<TW, TH, OX, OY>::kThreads * S, smem, stream>>>(src, dst, weights, spans, g, p, map,
+                                                                     on ? 1 : 0, on ? tma->err : nullptr);
     return cudaGetLastError();
 }
 
-template <int TW, int TH, int S, int OX = PX>
+template <int TW, int TH, int S, int OX = PX, int OY = 1>
 cudaError_t launch_nk(int nk, const float* src, float* dst, const float* weights,
                       const uint32_t* spans, const DirectGeometry& g, const StepParams& p,
                       cudaStream_t s, const DirectTma* tma, int buffer) {
     switch (nk) {
-    case 1: return launch_t<TW, TH, 1, S, OX>(src, dst, weights, spans, g, p, s, tma, buffer);
-    case 2: return launch_t<TW, TH, 2, S, OX>(src, dst, weights, spans, g, p, s, tma, buffer);
-    case 3: return launch_t<TW, TH, 3, S, OX>(src, dst, weights, spans, g, p, s, tma, buffer);
-    case 4: return launch_t<TW, TH, 4, S, OX>(src, dst, weights, spans, g, p, s, tma, buffer);
+    case 1: return launch_t<TW, TH, 1, S, OX, OY>(src, dst, weights, spans, g, p, s, tma, buffer);
+    case 2: return launch_t<TW, TH, 2, S, OX, OY>(src, dst, weights, spans, g, p, s, tma, buffer);
+    case 3: return launch_t<TW, TH, 3, S, OX, OY>(src, dst, weights, spans, g, p, s, tma, buffer);
+    case 4: return launch_t<TW, TH, 4, S, OX, OY>(src, dst, weights, spans, g, p, s, tma, buffer);
     default: return cudaErrorInvalidValue;
     }
 }
@@ -308,12 +368,23 @@ size_t direct_smem_bytes(int tile_cfg, int nk, const DirectGeometry& g) {
 cudaError_t launch_direct_step(int tile_cfg, int nk, const float* src, float* dst,
                                const float* weights, const uint32_t* spans,
                                const DirectGeometry& g, const StepParams& p,
-                               cudaStream_t stream, const DirectTma* tma, int buffer, int split, int ox) {
+                               cudaStream_t stream, const DirectTma* tma, int buffer, int split, int ox,
+                               int oy) {
+    if (oy != 1 && oy != 2) return cudaErrorInvalidValue;
+    if (oy == 2 && split != 1) return cudaErrorInvalidValue;
     if (ox == 16) {
         if (tile_cfg != kDirectTile64x32 || split != 1) return cudaErrorInvalidValue;
+        if (oy == 2) return launch_nk<64, 32, 1, 16, 2>(nk, src, dst, weights, spans, g, p, stream, tma, buffer);
         return launch_nk<64, 32, 1, 16>(nk, src, dst, weights, spans, g, p, stream, tma, buffer);
     }
     if (ox != PX) return cudaErrorInvalidValue;
+    if (oy == 2) {
+        if (tile_cfg == kDirectTile64x32)
+            return launch_nk<64, 32, 1, PX, 2>(nk, src, dst, weights, spans, g, p, stream, tma, buffer);
+        if (tile_cfg == kDirectTile64x16)
+            return launch_nk<64, 16, 1, PX, 2>(nk, src, dst, weights, spans, g, p, stream, tma, buffer);
+        return cudaErrorInvalidValue;
+    }
     if (tile_cfg == kDirectTile32x16) {
         switch (split) {
         case 1: return launch_nk<32, 16, 1>(nk, src, dst, weights, spans, g, p, stream, tma, buffer);

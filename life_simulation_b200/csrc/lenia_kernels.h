@@ -55,11 +55,15 @@ bool direct_tma_encode(int tile_cfg, const DirectGeometry& g, float* const field
 // wraps around the torus, keep the wrapped element loads.
 // `split` (1, or 2/4/8 with 32x16 tiles): kernel rows split over that many
 // thread groups per tile, for fields too small to fill the GPU otherwise.
-// `ox`: outputs per thread (8, or 16 with 64x32 tiles); the same bits.
+// `ox`: outputs per thread along x (8, or 16 with 64x32 tiles); `oy`: output
+// rows per thread (1, or 2 with 64x32 / 64x16 tiles and no split; its
+// per-row chunk spans must lie on the 8-tap grid that starts at -xp). The
+// same bits in every variant.
 cudaError_t launch_direct_step(int tile_cfg, int nk, const float* src, float* dst,
                                const float* weights, const uint32_t* spans,
                                const DirectGeometry& g, const StepParams& p, cudaStream_t stream,
-                               const DirectTma* tma = nullptr, int buffer = 0, int split = 1, int ox = 8);
+                               const DirectTma* tma = nullptr, int buffer = 0, int split = 1, int ox = 8,
+                               int oy = 1);
 // Extra shared memory of a split direct launch (the groups' partial sums).
 size_t direct_split_smem_bytes(int split, int nk);
 

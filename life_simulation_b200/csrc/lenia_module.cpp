@@ -768,7 +768,10 @@ int LeniaModule::buildDirectTables() {
             }
             uint32_t packed = 0;
             if (lo <= hi) {
-                const int start = (lo >= 0) ? (lo / 4) * 4 : -((-lo + 3) / 4) * 4;
+                // Chunks on the 8-tap grid that starts at dx = -xp (every row
+                // on one grid, so the two-rows-per-thread kernel can walk the
+                // union of two rows' spans; the extra taps weigh zero).
+                const int start = -dgeo_.xp + (lo + dgeo_.xp) / 8 * 8;
                 const int count = (hi - start + 1 + 7) / 8;
                 packed = uint32_t(start + 128) | (uint32_t(count) << 16);
             } else {
@@ -802,27 +805,47 @@ int LeniaModule::buildDirectTables() {
                                             direct_split_smem_bytes(direct_split_, direct_nk_) > 220 * 1024)
             direct_split_ /= 2;
     }
-    // Outputs per thread on 64x32 tiles: 8 or 16, whichever runs faster here
-    // (a few steps each on the context's own buffers; the same bits either way).
+    // Outputs per thread on large tiles: 8 or 16 along x (64x32 tiles) times 1
+    // or 2 rows (64x32 and 64x16 tiles, no split), whichever runs fastest here
+    // (a few steps each on the context's own buffers; the same bits in every
+    // variant). LENIA_DIRECT_OX ("8" / "16") and LENIA_DIRECT_OY ("1" / "2")
+    // at setup force either.
     direct_ox_ = 8;
-    const char* ox_env = std::getenv("LENIA_DIRECT_OX");  // "8" / "16" at setup: force either
+    direct_oy_ = 1;
+    const char* ox_env = std::getenv("LENIA_DIRECT_OX");
+    const char* oy_env = std::getenv("LENIA_DIRECT_OY");
     const int ox_forced = ox_env ? std::atoi(ox_env) : 0;
-    if (direct_tile_ == kDirectTile64x32 && ox_forced == 16) {
-        direct_ox_ = 16;
-    } else if (direct_tile_ == kDirectTile64x32 && ox_forced != 8) {
+    const int oy_forced = oy_env ? std::atoi(oy_env) : 0;
+    struct Shape {
+        int ox, oy;
+    };
+    std::vector<Shape> shapes;
+    const bool big = direct_tile_ == kDirectTile64x32 || direct_tile_ == kDirectTile64x16;
+    for (int ox : {8, 16})
+        for (int oy : {1, 2}) {
+            if (ox == 16 && direct_tile_ != kDirectTile64x32) continue;
+            if (oy == 2 && (!big || direct_split_ != 1)) continue;
+            if ((ox_forced == 8 || ox_forced == 16) && ox != ox_forced) continue;
+            if ((oy_forced == 1 || oy_forced == 2) && oy != oy_forced) continue;
+            shapes.push_back({ox, oy});
+        }
+    if (shapes.size() == 1) {
+        direct_ox_ = shapes[0].ox;
+        direct_oy_ = shapes[0].oy;
+    } else if (shapes.size() > 1) {
         StepParams p{};
         p.width = w_;
         p.height = h_;
         p.num_kernels = uint32_t(direct_nk_);
         for (int k = 0; k < 4; ++k) p.sigma[k] = 1.0f;
         cudaEvent_t a = takeEvent(), b = takeEvent();
-        float best[2] = {1e30f, 1e30f};
+        std::vector<float> best(shapes.size(), 1e30f);
         for (int rep = 0; rep < 3; ++rep)
-            for (int v = 0; v < 2; ++v) {
+            for (size_t v = 0; v < shapes.size(); ++v) {
                 cudaEventRecord(a, stream_);
                 for (int i = 0; i < 3; ++i)
                     launch_direct_step(direct_tile_, direct_nk_, field_[0], field_[1], d_weights_, d_spans_, dgeo_, p,
-                                       stream_, nullptr, 0, 1, v ? 16 : 8);
+                                       stream_, nullptr, 0, direct_split_, shapes[v].ox, shapes[v].oy);
                 cudaEventRecord(b, stream_);
                 cudaEventSynchronize(b);
                 float ms = 0.0f;
@@ -831,7 +854,11 @@ int LeniaModule::buildDirectTables() {
         event_pool_.push_back(a);
         event_pool_.push_back(b);
         if ((e = cudaGetLastError()) != cudaSuccess) return cudaFail(e, "direct shape choice");
-        if (best[1] < best[0]) direct_ox_ = 16;
+        size_t pick = 0;
+        for (size_t v = 1; v < shapes.size(); ++v)
+            if (best[v] < best[pick]) pick = v;
+        direct_ox_ = shapes[pick].ox;
+        direct_oy_ = shapes[pick].oy;
     }
     // Halo tiles by TMA where the size allows it (interior tiles only).
     // LENIA_DIRECT_TMA in the environment at setup: 0 keeps element loads,
@@ -860,7 +887,8 @@ int LeniaModule::buildDirectTables() {
                 cudaEventRecord(a, stream_);
                 for (int i = 0; i < 3; ++i)
                     launch_direct_step(direct_tile_, direct_nk_, field_[0], field_[1], d_weights_, d_spans_, dgeo_, p,
-                                       stream_, v ? &direct_tma_ : nullptr, 0, direct_split_, direct_ox_);
+                                       stream_, v ? &direct_tma_ : nullptr, 0, direct_split_, direct_ox_,
+                                       direct_oy_);
                 cudaEventRecord(b, stream_);
                 cudaEventSynchronize(b);
                 float ms = 0.0f;
@@ -1298,7 +1326,7 @@ int LeniaModule::stepImpl(const lenia_frame_params& fp, uint32_t substeps, cudaS
         } else {
             e = launch(LENIA_PHASE_DIRECT, s, [&] {
                 return launch_direct_step(direct_tile_, direct_nk_, src, dst, d_weights_, d_spans_, dgeo_, p, s,
-                                          &direct_tma_, cur_, direct_split_, direct_ox_);
+                                          &direct_tma_, cur_, direct_split_, direct_ox_, direct_oy_);
             });
             if (e != cudaSuccess) return cudaFail(e, "direct step");
         }
@@ -1320,6 +1348,7 @@ void LeniaModule::info(lenia_info* o) const {
     o->direct_tma = (!use_fft_ && direct_tma_.on) ? 1u : 0u;
     o->direct_split = use_fft_ ? 0u : uint32_t(direct_split_);
     o->direct_outputs_per_thread = use_fft_ ? 0u : uint32_t(direct_ox_);
+    o->direct_rows_per_thread = use_fft_ ? 0u : uint32_t(direct_oy_);
     o->direct_taps = use_fft_ ? 0u : direct_taps_;
     if (use_fft_) {
         for (int i = 0; i < fgeo_.row.npass && i < 8; ++i) o->fft_radix_row[i] = uint32_t(fgeo_.row.radix[i]);

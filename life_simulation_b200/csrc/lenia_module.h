@@ -206,6 +206,7 @@ private:
     int direct_nk_ = 1;
     int direct_split_ = 1;  // kernel-row thread groups per tile (small fields)
     int direct_ox_ = 8;     // outputs per thread (16: large tiles, when faster)
+    int direct_oy_ = 1;     // output rows per thread (2: large tiles, when faster)
     uint32_t direct_taps_ = 0;  // nonzero taps over the direct path's kernels
     FftGeometry fgeo_{};
     bool fast_col_ = false, fast_row_ = false;  // compile-time-plan passes

@@ -360,6 +360,40 @@ def test_direct_outputs_per_thread_give_the_same_bits(monkeypatch):
     np.testing.assert_array_equal(out[0], out[1])
 
 
+@pytest.mark.parametrize("w,h,conv,radius", [(1920, 1080, "directMulti", 24), (1280, 720, "direct", 32),
+                                             (1920, 1080, "direct", 13), (1024, 512, "direct", 7)])
+def test_direct_two_rows_per_thread_same_bits(monkeypatch, w, h, conv, radius):
+    """Two output rows per thread (each staged input chunk feeding two kernel
+    rows) against one row per thread, for both outputs-per-thread widths
+    where the tile allows them: the same bits (every output sums its taps in
+    the same order; the union of two rows' chunk spans adds exact zeros)."""
+    p = wl.fft3_params(w, h, conv=conv) if conv == "directMulti" else {"radius": radius, "dt": 0.2,
+                                                                       "growthMode": 0}
+    p["radius"] = radius
+    p["noiseAmount"] = 0.05
+    init = wl.patches(w, h, 12, 96, seed=8)
+    out = {}
+    for ox in ("8", "16"):
+        for oy in ("1", "2"):
+            monkeypatch.setenv("LENIA_DIRECT_OX", ox)
+            monkeypatch.setenv("LENIA_DIRECT_OY", oy)
+            m = lb.LeniaModule(p, w, h)
+            info = m.info()
+            if (info["direct_outputs_per_thread"], info["direct_rows_per_thread"]) != (int(ox), int(oy)):
+                m.close()
+                continue  # the tile this size gets has no such variant
+            m.reset(3)
+            m.upload(init)
+            for f in range(2):
+                m.encode(f, 2)
+            out[(ox, oy)] = m.field()
+            m.close()
+    assert ("8", "2") in out, "two rows per thread never ran"
+    ref = out[("8", "1")]
+    for k, v in out.items():
+        np.testing.assert_array_equal(v, ref, err_msg=str(k))
+
+
 def test_direct_tma_off_for_unaligned_widths():
     m = lb.LeniaModule({"radius": 5}, 37, 23)  # row stride not a multiple of 16 bytes
     assert m.info()["direct_tma"] is False
