@@ -137,4 +137,6 @@ def workload(name: str):
         return fft3_params(1920, 1080), 1920, 1080, patches(1920, 1080, 20, 96, seed=2)
     if name == "fft3_1024x512":
         return fft3_params(1024, 512), 1024, 512, patches(1024, 512, 20, 96, seed=2)
+    if name == "direct_720p_r32":  # the reference's published direct configuration (one kernel, R=32)
+        return {"radius": 32, "convMode": "direct"}, 1280, 720, patches(1280, 720, 12, 96, seed=2)
     raise KeyError(name)
