@@ -174,9 +174,10 @@ __global__ void __launch_bounds__(ColK<PF, B, SPLIT>::T)
             }
         }
         if (k0 == 0) __syncthreads();  // c0 (packed DC/Nyquist column) visible
-        for (int kk = 0; kk < nk; ++kk) {
-            // Spectrum product, then the inverse's first pass (radix RL, no
-            // twiddles) from registers into Y.
+        // Spectrum product of kernel kk, then the inverse's first pass (radix
+        // RL, no twiddles) from registers into Y; kernel kk+1's spectrum values
+        // are fetched while kk's remaining passes run.
+        const auto first_inverse = [&](int kk) {
 #pragma unroll
             for (int it = 0; it < K::ITL; ++it) {
                 if (!ok[it]) continue;
@@ -208,14 +209,31 @@ __global__ void __launch_bounds__(ColK<PF, B, SPLIT>::T)
                 for (int t = 0; t < RL; ++t) Y[bi[it] * PITCH + jj[it] * RL + t] = D[t];
             }
             if (kk + 1 < nk) fetch_k(kk + 1);
-            __syncthreads();
-            float2* Z = mid_passes<PI, 1, PI::np - 1, true, B, T, PITCH>(Y, X, twi, cols);
+        };
+        // The inverse's last pass of kernel kk from Z into U_kk.
+        const auto last_inverse = [&](int kk, const float2* Z) {
             float2* dst = U + size_t(kk) * M * H + gbase;
             pass_gen<PI, PI::np - 1, true, B, T>(
                 [&](int b, int i) { return Z[b * PITCH + i]; },
                 [&](int b, int i, float2 v) { dst[size_t(i) * KB + b] = v; }, twi, cols);
-            __syncthreads();
+        };
+        // With an odd number of middle passes the last pass reads X while the
+        // next kernel's first pass writes Y, so the two share one barrier
+        // interval: the last pass's threads (radix 15 at 1080: 288 of 544)
+        // are joined by the whole CTA's next first pass instead of idling at
+        // a barrier. Same operations, same bits.
+        constexpr bool kMerge = (PI::np - 2) % 2 == 1;
+        if (nk > 0) first_inverse(0);
+        for (int kk = 0; kk < nk; ++kk) {
+            __syncthreads();  // Y holds kernel kk's first pass
+            float2* Z = mid_passes<PI, 1, PI::np - 1, true, B, T, PITCH>(Y, X, twi, cols);
+            last_inverse(kk, Z);
+            if (kk + 1 < nk) {
+                if constexpr (!kMerge) __syncthreads();  // Z is Y: read before it is rewritten
+                first_inverse(kk + 1);
+            }
         }
+        __syncthreads();
     }
 }
 
@@ -317,14 +335,19 @@ __global__ void __launch_bounds__(RowK<PI, RB, SPLIT>::T,
         for (int kk = 0; kk < nk; ++kk) {
             float2* cur = stg[(base + kk) & 1];
             if constexpr (PIPE) {
+                // One barrier makes item kk's rows visible and frees the
+                // other staging buffer (item kk-1's, whose last pass every
+                // thread has finished); item kk+1 then lands there while kk
+                // is transformed.
+                cp_async_wait_all();
+                __syncthreads();
                 stage(stg[(base + kk + 1) & 1], y0, kk + 1);
                 cp_async_commit();
-                cp_async_wait_prev();
             } else {
                 stage(cur, y0, kk);
                 cp_async_wait_all();
+                __syncthreads();
             }
-            __syncthreads();
             // Inverse of the real-FFT split folded into the first pass's loads.
             pass_gen<PI, 0, true, RB, T>([&](int b, int i) { return c2r_split<M>(cur + b * PITCH, twr, i); },
                                          [&](int b, int i, float2 v) { bw[b * PITCH + i] = v; }, twi, rows);
@@ -364,20 +387,21 @@ __global__ void __launch_bounds__(RowK<PI, RB, SPLIT>::T,
                     acc[it][t][1] = kk == 0 ? c1 : acc[it][t][1] + c1;
                 }
             }
-            __syncthreads();
+            if constexpr (!PIPE) __syncthreads();  // cur (the one staging buffer) read
         }
         // The rows of A are in sA; the other staging buffer takes the next
         // row group's first item.
         float2* sA = stg[(base + nk) & 1];
         if constexpr (PIPE) {
+            cp_async_wait_all();
+            __syncthreads();  // A's rows visible; the last kernel's buffer free
             stage(stg[(base + nk + 1) & 1], y0 + int(gridDim.x) * RB, 0);
             cp_async_commit();
-            cp_async_wait_prev();
         } else {
             stage(sA, y0, nk);
             cp_async_wait_all();
+            __syncthreads();
         }
-        __syncthreads();
         // Euler step, noise, injection, clip (or, with nk == 0, the field as
         // is); the result is kept for the forward row transform (first
         // pass radix RC, the same elements per thread).
