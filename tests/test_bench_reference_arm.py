@@ -44,3 +44,23 @@ def test_reference_arm_other_ranks_exit_quietly():
     p = run_bench({"RANK": "1", "WORLD_SIZE": "2", "LOCAL_RANK": "1"}, "--steps", "2", "--warmup", "1")
     assert p.returncode == 0, p.stderr[-2000:]
     assert p.stdout.strip() == ""
+
+
+def test_traffic_comes_only_from_a_named_capture(tmp_path, monkeypatch):
+    """roofline.traffic is the DRAM traffic of an ncu capture of the same
+    workload, with its command as the source; absent, another workload or an
+    unreadable file: null, never a constant."""
+    sys.path.insert(0, ROOT)
+    import bench
+
+    f = tmp_path / "traffic.json"
+    monkeypatch.setattr(bench, "TRAFFIC_FILE", str(f))
+    assert bench.captured_traffic("row_growth", "fft3_1080p") == (None, None)
+    f.write_text(json.dumps({"workload": "fft3_1080p", "command": "ncu ... bench.py", "note": "one launch",
+                             "kernels": {"row_growth": {"dram_bytes_per_launch": 123}}}))
+    t, src = bench.captured_traffic("row_growth", "fft3_1080p")
+    assert t == 123 and "ncu ... bench.py" in src
+    assert bench.captured_traffic("column", "fft3_1080p") == (None, None)
+    assert bench.captured_traffic("row_growth", "single_256") == (None, None)
+    f.write_text("{not json")
+    assert bench.captured_traffic("row_growth", "fft3_1080p") == (None, None)
