@@ -45,6 +45,32 @@ struct DirectTile {
     static constexpr int kThreads = (TW / OX) * (TH / OY);
 };
 
+// Shared memory serves a warp's 16-byte loads eight lanes at a time; a
+// phase of eight lanes is conflict-free when its lanes hit eight different
+// 16-byte bank quads. A thread reads its inputs OX floats to the right of its
+// x-neighbour's and one tile row (TP floats) below its y-neighbour's. So the
+// halo tile's row pitch is 4 modulo 8 floats (consecutive rows start on
+// bank quads of opposite parity), and each phase holds 32 / OX threads along
+// x (distinct quads within a row) times 8 OX / 32 rows.
+__host__ __device__ constexpr int tile_pitch(int tw, int xp) { return tw + 2 * xp + 12; }
+
+// Thread lt of a tile group (TW / OX threads per output row): its thread
+// column tx and output row within the tile, lanes ordered so every phase of
+// eight lanes is two or four threads along x by four or two rows. The
+// mapping only changes which thread computes which outputs.
+template <int TW, int OX>
+__device__ __forceinline__ void tile_thread(int lt, int& tx, int& row) {
+    constexpr int NX = TW / OX;           // threads along x
+    constexpr int XP = 32 / OX;           // threads along x in one phase (2 or 4)
+    constexpr int RP = 8 / XP;            // rows in one phase
+    constexpr int XH = NX / XP;           // phases along x in one warp
+    constexpr int RW = 32 / NX;           // rows per warp
+    static_assert(NX % XP == 0 && 32 % NX == 0, "tile width and outputs per thread");
+    const int lane = lt & 31, phase = lane >> 3;
+    tx = lane % XP + XP * (phase % XH);
+    row = (lt >> 5) * RW + (lane / XP) % RP + RP * (phase / XH);
+}
+
 // Per-kernel-row chunk plan, filled on the host: for row dy (0..2R), the first
 // 8-tap chunk starts at dx = start (relative to -XP... see host) and `count`
 // chunks follow. Packed as (start + 128) | (count << 16).
@@ -104,7 +130,7 @@ __device__ __forceinline__ void direct_tile(const float* __restrict__ src, float
                                             const CUtensorMap* tmap, int* err) {
     extern __shared__ __align__(128) float smem[];
     __shared__ __align__(8) uint64_t tma_bar;
-    const int TP = TW + 2 * g.xp + 8;          // tile pitch (floats), multiple of 4
+    const int TP = tile_pitch(TW, g.xp);       // tile pitch (floats), 4 modulo 8
     const int TR = TH + 2 * g.r;               // tile rows
     float* tile = smem;                        // [TR][TP]
     float* wts = tile + TR * TP;               // [NK][2R+1][WP]
@@ -163,7 +189,9 @@ __device__ __forceinline__ void direct_tile(const float* __restrict__ src, float
     }
     __syncthreads();
 
-    const int tx = lt % (TW / OX), ty = lt / (TW / OX) * OY;  // ty: first output row within the tile
+    int tx, ty;  // thread column; first output row within the tile
+    tile_thread<TW, OX>(lt, tx, ty);
+    ty *= OY;
     const int ox = tx * OX;  // first output column within the tile
     float acc[OY][NK][OX];
 #pragma unroll
@@ -318,7 +346,7 @@ template <int TW, int TH, int NK, int S, int OX, int OY>
 cudaError_t launch_t(const float* src, float* dst, const float* weights, const uint32_t* spans,
                      const DirectGeometry& g, const StepParams& p, cudaStream_t stream, const DirectTma* tma,
                      int buffer) {
-    const int TP = TW + 2 * g.xp + 8;
+    const int TP = tile_pitch(TW, g.xp);
     const size_t smem = sizeof(float) * (size_t(TH + 2 * g.r) * TP + size_t(NK) * g.ksize * g.wp) +
                         sizeof(uint32_t) * NK * g.ksize +
                         sizeof(float) * size_t(S - 1) * NK * DirectTile<TW, TH, OX, OY>::kThreads * OX;
@@ -360,7 +388,7 @@ void tile_shape(int tile_cfg, int& TW, int& TH) {
 size_t direct_smem_bytes(int tile_cfg, int nk, const DirectGeometry& g) {
     int TW, TH;
     tile_shape(tile_cfg, TW, TH);
-    const int TP = TW + 2 * g.xp + 8;
+    const int TP = tile_pitch(TW, g.xp);
     return sizeof(float) * (size_t(TH + 2 * g.r) * TP + size_t(nk) * g.ksize * g.wp) +
            sizeof(uint32_t) * nk * g.ksize;
 }
@@ -410,7 +438,7 @@ bool direct_tma_encode(int tile_cfg, const DirectGeometry& g, float* const field
     out.on = false;
     int TW, TH;
     tile_shape(tile_cfg, TW, TH);
-    const int TP = TW + 2 * g.xp + 8, TR = TH + 2 * g.r;
+    const int TP = tile_pitch(TW, g.xp), TR = TH + 2 * g.r;
     // Row stride a multiple of 16 bytes; the box within the field and within
     // the 256-element limit per dimension; its rows a multiple of 16 bytes.
     if (w % 4 != 0 || TP > 256 || TR > 256 || TP > w || TR > h || (TP * 4) % 16 != 0) return false;
