@@ -907,7 +907,6 @@ def tc_bench(warmup: int = 3, steps: int = 64, error_check: bool = True) -> dict
     # x 128 FLOP (real 32x32 GEMM per 16 points) x 3 (hi/lo), per column.
     tc_flops = (1 + K) * 3 * h * 128 * 3 * (w // 2)
     res = {}
-    state = init
     for prec in ("fp32", "fp16x3", "bf16x3"):
         p = wl.fft3_params(w, h)
         p["radius"] = 32
@@ -944,8 +943,7 @@ def tc_bench(warmup: int = 3, steps: int = 64, error_check: bool = True) -> dict
         if error_check:
             # One step from the seeded field itself (alive; the timed steps
             # have let the patches decay by now).
-            state = init
-            m.upload(state)
+            m.upload(init)
             fp.frame_index = fp.audio_frame = 0
             m.step(fp, 1, sh)
             torch.cuda.synchronize()
@@ -958,9 +956,9 @@ def tc_bench(warmup: int = 3, steps: int = 64, error_check: bool = True) -> dict
         p["radius"] = 32
         o = lo.OracleLenia(p, w, h, "f64")
         o.reset(2)
-        o.set_initial_field(state)
+        o.set_initial_field(init)
         o.encode(0)  # builds the kernels; its state is replaced below
-        o.state = state.astype(np.float64)
+        o.state = init.astype(np.float64)
         o.step_once(o.frame_params(), lo.pcg_hash(o.seed_), 0, 0)
         for prec, r in res.items():
             d = r.pop("_next").astype(np.float64) - o.state
