@@ -281,7 +281,7 @@ __global__ void __launch_bounds__(RowK<PI, RB>::T, (512 / RowK<PI, RB>::T > 1 ? 
             }
             __syncthreads();
             float2* Y = mid_passes<PF, 1, PF::np - 1, false, RB, T, PITCH>(ba, bb, twf, rows);
-            float2* Zo = (Y == ba) ? bb : ba;
+            float2* Zo = (PF::np - 2) % 2 ? ba : bb;  // the other buffer, chosen at compile time (shared accesses)
             pass_gen<PF, PF::np - 1, false, RB, T>([&](int b, int i) { return Y[b * PITCH + i]; },
                                                     [&](int b, int i, float2 v) { Zo[b * PITCH + i] = v; }, twf,
                                                     rows);

@@ -157,7 +157,11 @@ __global__ void __launch_bounds__(ColK<PF, B, SPLIT>::T)
             __syncthreads();
         }
         float2* X = mid_passes<PF, 1, PF::np - 1, false, B, T, PITCH>(ba, bb, twf, cols);
-        float2* Y = (X == ba) ? bb : ba;
+        // The other buffer, chosen by the (compile-time) pass count rather than
+        // by comparing pointers, so every access through it stays a
+        // shared-memory access (a runtime select between buffers compiles to
+        // generic loads and stores).
+        float2* Y = (PF::np - 2) % 2 ? ba : bb;
         // Last forward pass: the column spectrum C stays in registers.
         float2 C[K::ITL][RL];
 #pragma unroll
@@ -282,7 +286,10 @@ __global__ void __launch_bounds__(RowK<PI, RB, SPLIT>::T,
     float2* twi = twr + (M + 1);
     float2* twf = twi + PI::tw_size();
     // Staging (16-byte aligned) and work buffers.
-    float2* stg[2] = {sm + K::BUF0, sm + K::BUF0 + (PIPE ? RB * PITCH : 0)};
+    // Staging buffer i & 1 by address arithmetic on the shared array (a
+    // runtime-indexed pointer table would make every access through it a
+    // generic load).
+    const auto stg = [&](int i) { return sm + K::BUF0 + (PIPE ? (i & 1) * (RB * PITCH) : 0); };
     float2* bw = sm + K::BUF0 + (PIPE ? 2 : 1) * RB * PITCH;
     copy_table(twr, twr_g, M + 1);
     copy_table(twi, twi_g, PI::tw_size());
@@ -315,7 +322,7 @@ __global__ void __launch_bounds__(RowK<PI, RB, SPLIT>::T,
     };
     int base = 0;  // staging buffer of the group's first item
     if constexpr (PIPE) {
-        stage(stg[0], int(blockIdx.x) * RB, 0);
+        stage(stg(0), int(blockIdx.x) * RB, 0);
         cp_async_commit();
     }
     if (int(blockIdx.x) * RB >= H) allow_dependents();
@@ -333,7 +340,7 @@ __global__ void __launch_bounds__(RowK<PI, RB, SPLIT>::T,
         }
         float acc[K::ITL][RC][2];
         for (int kk = 0; kk < nk; ++kk) {
-            float2* cur = stg[(base + kk) & 1];
+            float2* cur = stg(base + kk);
             if constexpr (PIPE) {
                 // One barrier makes item kk's rows visible and frees the
                 // other staging buffer (item kk-1's, whose last pass every
@@ -341,7 +348,7 @@ __global__ void __launch_bounds__(RowK<PI, RB, SPLIT>::T,
                 // is transformed.
                 cp_async_wait_all();
                 __syncthreads();
-                stage(stg[(base + kk + 1) & 1], y0, kk + 1);
+                stage(stg(base + kk + 1), y0, kk + 1);
                 cp_async_commit();
             } else {
                 stage(cur, y0, kk);
@@ -391,11 +398,11 @@ __global__ void __launch_bounds__(RowK<PI, RB, SPLIT>::T,
         }
         // The rows of A are in sA; the other staging buffer takes the next
         // row group's first item.
-        float2* sA = stg[(base + nk) & 1];
+        float2* sA = stg(base + nk);
         if constexpr (PIPE) {
             cp_async_wait_all();
             __syncthreads();  // A's rows visible; the last kernel's buffer free
-            stage(stg[(base + nk + 1) & 1], y0 + int(gridDim.x) * RB, 0);
+            stage(stg(base + nk + 1), y0 + int(gridDim.x) * RB, 0);
             cp_async_commit();
         } else {
             stage(sA, y0, nk);
@@ -445,7 +452,7 @@ __global__ void __launch_bounds__(RowK<PI, RB, SPLIT>::T,
         }
         __syncthreads();
         float2* Y = mid_passes<PF, 1, PF::np - 1, false, RB, T, PITCH>(bw, sA, twf, rows);
-        float2* Zo = (Y == bw) ? sA : bw;
+        float2* Zo = (PF::np - 2) % 2 ? bw : sA;  // the other buffer (see the column pass)
         pass_gen<PF, PF::np - 1, false, RB, T>([&](int b, int i) { return Y[b * PITCH + i]; },
                                                 [&](int b, int i, float2 v) { Zo[b * PITCH + i] = v; }, twf, rows);
         __syncthreads();
