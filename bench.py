@@ -985,17 +985,21 @@ def run_tc(args):
     return 0
 
 
-def sweep_batched(worlds, inits):
+def sweep_batched(worlds, inits, form=None):
     """The 512-world sweep's batched form on this GPU: the batch's graphs
     replay 4 x 60 substeps with the activity readback after each (the lab's
-    luma statistic per world). Returns (wall seconds, per-readback activity,
-    path per world)."""
+    luma statistic per world). `form`: the launch form (None: the one the
+    batch's autotuner picks). Returns (wall seconds, per-readback activity,
+    path per world, launch form used)."""
     import torch
 
     import life_simulation_b200 as lb
     from life_simulation_b200.sweep import is_alive
 
     b = lb.LeniaBatch(worlds, lb.BATCH_AUTO)
+    if form is not None:
+        b.set_launch_form(form)
+    used = b.launch_form()
     for i, a in enumerate(inits):
         b.upload(i, a)
     b.step(60)  # warm-up (also captures the graph)
@@ -1019,7 +1023,7 @@ def sweep_batched(worlds, inits):
                 for j, (mean, std) in enumerate(acts)]
     paths = [b.path(i) for i in range(len(worlds))]
     b.close()
-    return seconds, activity, paths
+    return seconds, activity, paths, used
 
 
 def sweep_worlds(specs):
@@ -1043,7 +1047,17 @@ def sweep_bench(plain_steps: int = 10) -> dict:
     specs, inits = wl.sweep512()
     worlds = sweep_worlds(specs)
     px = sum(w.width * w.height for w in worlds)
-    batched_s, activity, paths = sweep_batched(worlds, inits)
+    batched_s, activity, paths, form = sweep_batched(worlds, inits)
+    # The other launch form, timed the same way, for comparison.
+    other = lb.BATCH_FORM_PER_SIZE if form == lb.BATCH_FORM_PERSISTENT else lb.BATCH_FORM_PERSISTENT
+    try:
+        other_s = sweep_batched(worlds, inits, other)[0]
+    except lb.LeniaError:
+        other_s = None
+    names = {lb.BATCH_FORM_PERSISTENT: "persistent", lb.BATCH_FORM_PER_SIZE: "per_size"}
+    forms = {names[form]: px * 240 / batched_s / 1e6}
+    if other_s:
+        forms[names[other]] = px * 240 / other_s / 1e6
     mods = []
     for i, w in enumerate(worlds):
         conv = "fft" if paths[i] == lb.CONV_FFT else "direct"
@@ -1069,6 +1083,9 @@ def sweep_bench(plain_steps: int = 10) -> dict:
     return {"value": batched, "unit": UNIT, "plain": plain, "speedup": batched / plain,
             "worlds": len(worlds), "pixels_per_step": px, "steps": 240,
             "direct_worlds": paths.count(lb.CONV_DIRECT), "fft_worlds": paths.count(lb.CONV_FFT),
+            "launch_form": names[form], "forms": forms,
+            "launches_per_substep": {"persistent": 1,
+                                     "per_size": 2 * len({(w.width, w.height) for w in worlds}) + 1},
             "activity": activity,
             "timing": "wall clock incl. 4 activity readbacks (batched); plain: "
                       f"{plain_steps} substeps per world, worlds in sequence on one stream"}
@@ -1101,7 +1118,7 @@ def run_sweep(args):
     shares = partition(costs, world)
     mine = shares[rank]
     torch.distributed.barrier()
-    batched_s, _, paths = sweep_batched(sweep_worlds([specs[i] for i in mine]), [inits[i] for i in mine])
+    batched_s, _, paths, _ = sweep_batched(sweep_worlds([specs[i] for i in mine]), [inits[i] for i in mine])
     t = torch.tensor([batched_s], device="cuda", dtype=torch.float64)
     torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
     batched_s = float(t.item())

@@ -288,9 +288,14 @@ int lenia_step_render(lenia_ctx* ctx, const lenia_frame_params* fp, uint32_t sub
  * (Apps/LifePresetLab/main.cpp:718-795, a SceneRunner per variant): n
  * independent worlds of any sizes and parameters, each a single-ring Lenia
  * (the direct module's kernel, Lenia.cpp:410-446), stepped together. A
- * substep of the whole batch is one direct launch over every direct world
- * plus one column and one row launch per field size with spectral worlds;
- * lenia_batch_step replays k substeps as one captured CUDA graph. The path of
+ * substep of the whole batch is either one persistent launch over a work
+ * list of every world's column groups, direct tiles and row groups (where
+ * every spectral world's size has a persistent body: heights 64, 128, 216,
+ * 256, 512, 1024 and widths 128, 256, 384, 512, 1024), or one direct launch
+ * over every direct world plus one column and one row launch per field size
+ * with spectral worlds; creation times both and keeps the faster
+ * (lenia_batch_launch_form). lenia_batch_step replays k substeps as one
+ * captured CUDA graph. The path of
  * each world is chosen at creation: LENIA_BATCH_AUTO times the direct and
  * spectral passes on the batch's own buffers and gives each world the
  * cheaper one. Each world evolves exactly as it would alone. */
@@ -326,8 +331,20 @@ int lenia_batch_init_noise(lenia_batch* b, uint32_t world, uint32_t seed, float 
  * luma 0.2126 R + 0.7152 G + 0.0722 B of the world's RGBA16F colour layer
  * through palette `cm` (n doubles each). */
 int lenia_batch_activity(lenia_batch* b, const lenia_colormap* cm, double* mean_luma, double* stddev_luma);
+/* Waits for the batch's work. LENIA_ERR_CUDA also when, in the persistent
+ * form, a row group's bounded wait for its world's column groups ran out
+ * (a device fault elsewhere; those rows were left unwritten). */
 int lenia_batch_sync(lenia_batch* b);
 const char* lenia_batch_last_message(lenia_batch* b);
+/* Launch form of a substep (extension; the reference runs one variant at a
+ * time): LENIA_BATCH_FORM_PERSISTENT (one launch) or
+ * LENIA_BATCH_FORM_PER_SIZE, as chosen at creation (LENIA_BATCH_PERSISTENT=0/1
+ * in the environment forces it). lenia_batch_set_launch_form switches it
+ * (LENIA_ERR_UNSUPPORTED when some spectral size has no persistent body);
+ * both forms give the same fields. */
+enum { LENIA_BATCH_FORM_PER_SIZE = 0, LENIA_BATCH_FORM_PERSISTENT = 1 };
+int lenia_batch_launch_form(lenia_batch* b, uint32_t* form);
+int lenia_batch_set_launch_form(lenia_batch* b, uint32_t form);
 
 /* ---- One spectral substep without device allocation ----
  * No counterpart in the reference (its module always owns its textures).

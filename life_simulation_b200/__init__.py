@@ -110,7 +110,7 @@ EXPORTS = (
     "lenia_bus_last_message", "lenia_create_scene_module", "lenia_attach_bus",
     "lenia_get_colormap", "lenia_set_colormap", "lenia_colormap_from_json", "lenia_render_rgba16f",
     "lenia_step_render",
-    "lenia_batch_init_noise", "lenia_batch_activity",
+    "lenia_batch_init_noise", "lenia_batch_activity", "lenia_batch_launch_form", "lenia_batch_set_launch_form",
     "lenia_npy_write_f32", "lenia_npy_read_f32", "lenia_save_state", "lenia_load_state",
 )
 
@@ -152,6 +152,7 @@ class AdjointConfig(ctypes.Structure):
                 ("kernels", KernelDef * 4), ("steps", ctypes.c_uint32), ("checkpoint_every", ctypes.c_uint32)]
 
 BATCH_AUTO, BATCH_DIRECT, BATCH_FFT = 0, 1, 2
+BATCH_FORM_PER_SIZE, BATCH_FORM_PERSISTENT = 0, 1
 
 
 class World(ctypes.Structure):
@@ -261,6 +262,8 @@ def load_library(path: str = LIB_PATH):
     L.lenia_save_state.argtypes = [P, ctypes.c_char_p]
     L.lenia_load_state.argtypes = [P, ctypes.c_char_p]
     L.lenia_batch_activity.argtypes = [P, ctypes.POINTER(ColorMap), P, P]
+    L.lenia_batch_launch_form.argtypes = [P, ctypes.POINTER(u32)]
+    L.lenia_batch_set_launch_form.argtypes = [P, u32]
     for name in EXPORTS:
         getattr(L, name)  # raises AttributeError if the build lacks a symbol
     _LIB = L
@@ -625,6 +628,15 @@ class LeniaBatch:
         p = ctypes.c_uint32()
         self._check(self._L.lenia_batch_world_path(self._h, i, ctypes.byref(p)))
         return p.value
+
+    def launch_form(self) -> int:
+        """BATCH_FORM_PERSISTENT (one launch per substep) or BATCH_FORM_PER_SIZE."""
+        f = ctypes.c_uint32()
+        self._check(self._L.lenia_batch_launch_form(self._h, ctypes.byref(f)))
+        return f.value
+
+    def set_launch_form(self, form: int) -> None:
+        self._check(self._L.lenia_batch_set_launch_form(self._h, form))
 
 
 def single_world_params(w: World, conv: str) -> dict:

@@ -3,14 +3,18 @@
 // the reference sweeps variants one SceneRunner at a time,
 // Apps/LifePresetLab/main.cpp:718-795).
 //
-// Per substep the whole batch is a handful of launches regardless of the
-// number of worlds: one direct launch over a flat tile list of every world
-// that the autotuner gave the direct path, and for each field size that has
-// spectral worlds one column-pass and one row-pass launch over a world table
-// (blockIdx.y = world). A tiny kernel then advances every world's substep
-// seed and frame index on the device, so a CUDA graph captured once replays
-// any number of substeps. Worlds never interact; a world's result is the
-// same as stepping it alone through a single-world context.
+// Two launch forms of a substep, whichever the autotuner measures faster:
+//   * persistent (lenia_batch_persistent.cu): ONE launch over a device work
+//     list of every world's column groups, direct tiles and row groups; row
+//     groups wait on per-world counters for their world's column groups, and
+//     the last CTA advances every world's substep seed and frame index;
+//   * per size: one direct launch over a flat tile list of every direct
+//     world, and for each field size with spectral worlds one column-pass and
+//     one row-pass launch over a world table (blockIdx.y = world), then a tiny
+//     kernel advances the seeds and frame indices.
+// Either way a CUDA graph captured once replays any number of substeps.
+// Worlds never interact; a world's result is the same as stepping it alone
+// through a single-world context.
 //
 // Path choice (the autotuner): at creation the direct kernel's cost per
 // pixel-tap and each size's spectral-step cost per pixel are measured on the
@@ -19,6 +23,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -155,6 +160,17 @@ struct BatchContext {
     int* d_npx = nullptr;
     double* d_stats = nullptr;
 
+    // The persistent form (lenia_batch_persistent.cu): one launch per
+    // substep over a work list per parity; usable when every spectral world's
+    // size has a persistent body. `persistent` is the form in use.
+    bool persist_ok = false, persistent = false;
+    PersistItem* d_items[2] = {nullptr, nullptr};
+    int nitems = 0;
+    uint32_t* d_ctl = nullptr;  // 2 counter sets of kPersistCtlHead + n words
+    int* d_err = nullptr;       // set when a row item's wait ran out
+    size_t persist_smem = 0;
+    int persist_grid_n = 0;
+
     // Captured graphs by substep count and parity.
     std::map<std::pair<uint32_t, int>, cudaGraphExec_t> graphs;
     std::vector<void*> allocs;
@@ -172,15 +188,24 @@ struct BatchContext {
         if (stream) cudaStreamDestroy(stream);
     }
 
-    float* field(int w, int half) { return fields + field_off[size_t(w)] + size_t(half) * worlds[w].width * worlds[w].height; }
+    // Each field starts on a 256-byte boundary (the row passes stage fields
+    // with 16-byte asynchronous copies; a world of odd size before it must
+    // not shift it).
+    static size_t field_stride(const lenia_world& w) { return (size_t(w.width) * w.height + 63) / 64 * 64; }
+    float* field(int w, int half) { return fields + field_off[size_t(w)] + size_t(half) * field_stride(worlds[w]); }
 
     int fail(int code, std::string m) {
         message = std::move(m);
         return code;
     }
 
-    cudaError_t launch_step(int parity, cudaStream_t s);
+    cudaError_t launch_step(int parity, cudaStream_t s, bool advance = true);
     cudaError_t launch_r2c(int parity, cudaStream_t s);
+    int build_persistent(const std::vector<int>& slot_of);
+    void drop_graphs() {
+        for (auto& g : graphs) cudaGraphExecDestroy(g.second);
+        graphs.clear();
+    }
 };
 
 namespace {
@@ -204,7 +229,13 @@ StepParams world_params(const lenia_world& w) {
 
 }  // namespace
 
-cudaError_t BatchContext::launch_step(int parity, cudaStream_t s) {
+// One substep of every world. The per-size form leaves the seed advance to
+// advance_kernel (launched by the caller); the persistent form does it in
+// its last CTA unless `advance` is false (timing).
+cudaError_t BatchContext::launch_step(int parity, cudaStream_t s, bool advance) {
+    if (persistent)
+        return launch_persistent(d_items[parity], nitems, d_ctl, int(worlds.size()), parity, d_param_loc, d_base_seed,
+                                 d_frame, advance, d_err, persist_smem, persist_grid_n, s);
     cudaError_t e = cudaSuccess;
     if (ntiles > 0) e = launch_direct_worlds(d_dtab[parity], d_tiles, ntiles, max_r, s);
     for (auto& c : classes) {
@@ -223,6 +254,90 @@ cudaError_t BatchContext::launch_r2c(int parity, cudaStream_t s) {
         e = launch_row_fast_worlds(c.H, c.M, c.t, c.tw_r2c, c.row_batch, c.d_r2c[parity], int(c.ids.size()), s);
     }
     return e;
+}
+
+// Work lists of the persistent form, one per table parity: every column
+// item (world by world, each world's groups in order), then the direct
+// tiles, then every row item in the same world order -- a row item comes
+// after all column items of its world, which is what its wait relies on.
+// Returns LENIA_OK with persist_ok false when some spectral size has no
+// persistent body.
+int BatchContext::build_persistent(const std::vector<int>& slot_of) {
+    persist_ok = false;
+    std::vector<int> col_h, row_m;
+    for (auto& c : classes) {
+        if (persist_col_group(c.H) == 0 || persist_row_group(c.M) == 0) return LENIA_OK;
+        col_h.push_back(c.H);
+        row_m.push_back(c.M);
+    }
+    const int n = int(worlds.size());
+    // Groups per item: several consecutive column (row) groups share one
+    // item's set-up (its descriptor, world entry and dependency check).
+    int per_item = 4;
+    if (const char* env = std::getenv("LENIA_PERSIST_GROUPS")) per_item = std::max(1, std::atoi(env));
+    std::vector<PersistItem> items[2];
+    for (int par = 0; par < 2; ++par) {
+        std::vector<PersistItem> cols, rows;
+        for (auto& c : classes) {
+            const int B = persist_col_group(c.H) * per_item, RB = persist_row_group(c.M) * per_item;
+            const int ncol = (c.M + B - 1) / B;
+            for (int wi : c.ids) {
+                PersistItem it{};
+                it.world = c.d_stab[par] + slot_of[size_t(wi)];
+                it.world_id = wi;
+                it.kind = kPersistCol;
+                it.count = per_item;
+                it.shape = c.H;
+                it.tw0 = c.t.col_twf;
+                it.tw1 = c.t.col_twi;
+                for (int g = 0; g < ncol; ++g) {
+                    it.group = g * B;
+                    cols.push_back(it);
+                }
+                it.kind = kPersistRow;
+                it.shape = c.M;
+                it.tw0 = c.t.row_twi;
+                it.tw1 = c.t.row_twf;
+                it.tw2 = c.tw_r2c;
+                it.need = ncol;
+                for (int y = 0; y < c.H; y += RB) {
+                    it.group = y;
+                    rows.push_back(it);
+                }
+            }
+        }
+        std::vector<PersistItem> direct;
+        for (int wi : direct_ids) {
+            const lenia_world& w = worlds[size_t(wi)];
+            PersistItem it{};
+            it.world = d_dtab[par] + slot_of[size_t(wi)];
+            it.world_id = wi;
+            it.kind = kPersistDirect;
+            for (int ty = 0; ty < (int(w.height) + 31) / 32; ++ty)
+                for (int tx = 0; tx < (int(w.width) + 63) / 64; ++tx) {
+                    it.group = tx | (ty << 16);
+                    direct.push_back(it);
+                }
+        }
+        items[par] = cols;
+        items[par].insert(items[par].end(), direct.begin(), direct.end());
+        items[par].insert(items[par].end(), rows.begin(), rows.end());
+    }
+    nitems = int(items[0].size());
+    if (nitems == 0) return LENIA_OK;
+    persist_smem = persist_smem_bytes(col_h, row_m, direct_ids.empty() ? 0 : max_r);
+    persist_grid_n = persist_grid(persist_smem);
+    if (persist_grid_n <= 0) return LENIA_OK;
+    for (int par = 0; par < 2; ++par) {
+        if (alloc(&d_items[par], items[par].size()) != cudaSuccess) return LENIA_ERR_CUDA;
+        cudaMemcpy(d_items[par], items[par].data(), items[par].size() * sizeof(PersistItem), cudaMemcpyHostToDevice);
+    }
+    if (alloc(&d_ctl, 2 * (size_t(kPersistCtlHead) + n)) != cudaSuccess || alloc(&d_err, 1) != cudaSuccess)
+        return LENIA_ERR_CUDA;
+    cudaMemset(d_ctl, 0, 2 * (size_t(kPersistCtlHead) + n) * sizeof(uint32_t));
+    cudaMemset(d_err, 0, sizeof(int));
+    persist_ok = true;
+    return LENIA_OK;
 }
 
 }  // namespace lenia
@@ -262,7 +377,7 @@ int lenia_batch_create(const lenia_world* worlds, uint32_t n, uint32_t policy, l
             if (w.width < 1 || w.height < 1 || !(w.sigma != 0.0f)) return LENIA_ERR_INVALID_ARG;
             if (w.radius > uint32_t(kMaxRadius) && (w.width % 2 || w.width < 2)) return LENIA_ERR_UNSUPPORTED;
             b.field_off[i] = total;
-            total += 2 * size_t(w.width) * w.height;
+            total += 2 * BatchContext::field_stride(w);
         }
         if ((e = b.alloc(&b.fields, total)) != cudaSuccess) return LENIA_ERR_CUDA;
         cudaMemsetAsync(b.fields, 0, total * sizeof(float), b.stream);
@@ -643,6 +758,52 @@ int lenia_batch_create(const lenia_world* worlds, uint32_t n, uint32_t policy, l
         cudaMemcpy(b.d_field_ptrs[1], fp1.data(), n * sizeof(float*), cudaMemcpyHostToDevice);
         cudaMemcpy(b.d_npx, npx.data(), n * sizeof(int), cudaMemcpyHostToDevice);
 
+        // Launch form: one persistent launch per substep where every spectral
+        // size has a persistent body, else (or when slower) the per-size
+        // launches. The autotuner times a few substeps of each on the batch's
+        // own buffers (no seed advance; the fields are cleared afterwards);
+        // LENIA_BATCH_PERSISTENT=0/1 forces the choice.
+        {
+            const int prc = b.build_persistent(slot_of);
+            if (prc < 0) return prc;
+            const char* env = std::getenv("LENIA_BATCH_PERSISTENT");
+            if (b.persist_ok && env && env[0] == '0' && env[1] == '\0') {
+                b.persistent = false;
+            } else if (b.persist_ok && env && env[0] == '1' && env[1] == '\0') {
+                b.persistent = true;
+            } else if (b.persist_ok) {
+                cudaEvent_t ea, eb;
+                cudaEventCreate(&ea);
+                cudaEventCreate(&eb);
+                float ms[2] = {0.0f, 0.0f};
+                for (int form = 0; form < 2; ++form) {
+                    b.persistent = form == 1;
+                    float best = 1e30f;
+                    for (int rep = 0; rep < 4; ++rep) {
+                        cudaEventRecord(ea, b.stream);
+                        cudaError_t r = cudaSuccess;
+                        for (int k = 0; k < 4 && r == cudaSuccess; ++k) r = b.launch_step(k & 1, b.stream, false);
+                        cudaEventRecord(eb, b.stream);
+                        cudaEventSynchronize(eb);
+                        float t = 0.0f;
+                        cudaEventElapsedTime(&t, ea, eb);
+                        if (r != cudaSuccess) t = 1e30f;
+                        if (rep > 0) best = std::min(best, t);
+                    }
+                    ms[form] = best;
+                }
+                cudaEventDestroy(ea);
+                cudaEventDestroy(eb);
+                b.persistent = ms[1] < ms[0];
+                cudaGetLastError();
+                cudaMemsetAsync(b.fields, 0, total * sizeof(float), b.stream);
+            }
+            if (b.persist_ok) {
+                cudaMemsetAsync(b.d_ctl, 0, 2 * (size_t(kPersistCtlHead) + n) * sizeof(uint32_t), b.stream);
+                cudaMemsetAsync(b.d_err, 0, sizeof(int), b.stream);
+            }
+        }
+
         cudaStreamSynchronize(b.stream);
         if ((e = cudaGetLastError()) != cudaSuccess) {
             b.message = std::string("batch setup: ") + cudaGetErrorString(e);
@@ -717,7 +878,7 @@ int lenia_batch_step(lenia_batch* bb, uint32_t steps, void* stream) {
             int par = b.cur;
             for (uint32_t k = 0; k < steps && e == cudaSuccess; ++k) {
                 e = b.launch_step(par, cap);
-                if (e == cudaSuccess) {
+                if (e == cudaSuccess && !b.persistent) {
                     advance_kernel<<<(n + 127) / 128, 128, 0, cap>>>(b.d_param_loc, n, b.d_base_seed, b.d_frame);
                     e = cudaGetLastError();
                 }
@@ -813,8 +974,50 @@ int lenia_batch_world_path(lenia_batch* bb, uint32_t world, uint32_t* path) {
 int lenia_batch_sync(lenia_batch* bb) {
     return lenia::abi_guard(bb ? &bb->ctx.message : nullptr, [&]() -> int {
         if (!bb) return LENIA_ERR_INVALID_ARG;
+        BatchContext& b = bb->ctx;
         cudaError_t e = cudaDeviceSynchronize();
-        return e == cudaSuccess ? LENIA_OK : bb->ctx.fail(LENIA_ERR_CUDA, cudaGetErrorString(e));
+        if (e != cudaSuccess) return b.fail(LENIA_ERR_CUDA, cudaGetErrorString(e));
+        if (b.d_err) {
+            int flag = 0;
+            e = cudaMemcpy(&flag, b.d_err, sizeof(int), cudaMemcpyDeviceToHost);
+            if (e != cudaSuccess) return b.fail(LENIA_ERR_CUDA, cudaGetErrorString(e));
+            if (flag) {
+                cudaMemset(b.d_err, 0, sizeof(int));
+                return b.fail(LENIA_ERR_CUDA,
+                              "persistent batch: a row item's wait for its world's column items ran out "
+                              "(those rows were not updated)");
+            }
+        }
+        return LENIA_OK;
+    });
+}
+
+int lenia_batch_launch_form(lenia_batch* bb, uint32_t* form) {
+    return lenia::abi_guard(bb ? &bb->ctx.message : nullptr, [&]() -> int {
+        if (!bb || !form) return LENIA_ERR_INVALID_ARG;
+        *form = bb->ctx.persistent ? LENIA_BATCH_FORM_PERSISTENT : LENIA_BATCH_FORM_PER_SIZE;
+        return LENIA_OK;
+    });
+}
+
+int lenia_batch_set_launch_form(lenia_batch* bb, uint32_t form) {
+    return lenia::abi_guard(bb ? &bb->ctx.message : nullptr, [&]() -> int {
+        if (!bb || form > LENIA_BATCH_FORM_PERSISTENT) return LENIA_ERR_INVALID_ARG;
+        BatchContext& b = bb->ctx;
+        if (form == LENIA_BATCH_FORM_PERSISTENT && !b.persist_ok)
+            return b.fail(LENIA_ERR_UNSUPPORTED, "no persistent body for some spectral world size of this batch");
+        const bool want = form == LENIA_BATCH_FORM_PERSISTENT;
+        if (want != b.persistent) {
+            // Graphs hold the other form's launches; the counter sets start clear.
+            cudaError_t e = cudaStreamSynchronize(b.stream);
+            if (e == cudaSuccess) e = cudaDeviceSynchronize();
+            if (e != cudaSuccess) return b.fail(LENIA_ERR_CUDA, cudaGetErrorString(e));
+            b.drop_graphs();
+            if (b.d_ctl)
+                cudaMemset(b.d_ctl, 0, 2 * (size_t(lenia::kPersistCtlHead) + b.worlds.size()) * sizeof(uint32_t));
+            b.persistent = want;
+        }
+        return LENIA_OK;
     });
 }
 

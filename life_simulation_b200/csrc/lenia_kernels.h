@@ -183,6 +183,43 @@ cudaError_t launch_col_fast_worlds(int H, int M, const FastTables& t, int batch,
 cudaError_t launch_row_fast_worlds(int H, int M, const FastTables& t, const float2* tw_r2c, int batch,
                                    const SpectralWorld* worlds, int n, cudaStream_t s);
 
+// One persistent launch per substep of a batch (lenia_batch_persistent.cu):
+// CTAs of kPersistThreads claim work items in list order; a row item waits
+// for its world's column items (a counter per world); the last CTA advances
+// every world's frame index and substep seed.
+constexpr int kPersistThreads = 256;
+constexpr int kPersistCtlHead = 32;  // counters per set before the per-world ones
+enum PersistKind { kPersistCol = 0, kPersistRow = 1, kPersistDirect = 2 };
+struct alignas(16) PersistItem {
+    const void* world;     // this parity's SpectralWorld (col/row) or DirectWorld entry
+    const float2* tw0;     // column: forward plan twiddles; row: inverse plan twiddles
+    const float2* tw1;     // column: inverse plan twiddles; row: forward plan twiddles
+    const float2* tw2;     // row: exp(-2 pi i k / W), k <= M
+    int kind;              // PersistKind
+    int shape;             // column: H; row: M (selects the compiled body)
+    int group;             // column: first column; row: first row; direct: tile x | tile y << 16
+    int world_id;          // the world's dependency counter
+    int need;              // row: column items of the world that precede it
+    int count;             // column / row: consecutive groups in this item (from `group` on)
+    int pad[2];
+};
+// Columns (rows) per item of the persistent bodies for a column length H
+// (half-spectrum width M); 0 when there is no body for that length.
+int persist_col_group(int H);
+int persist_row_group(int M);
+// Dynamic shared memory of a persistent launch whose items use these column
+// lengths, row lengths and direct halo radius (0: no direct items).
+size_t persist_smem_bytes(const std::vector<int>& col_h, const std::vector<int>& row_m, int direct_max_r);
+// Resident CTAs of the persistent kernel at that shared memory (0 on error).
+int persist_grid(size_t smem);
+// ctl: 2 counter sets of kPersistCtlHead + nworlds words, zero before the
+// first launch; launches alternate par 0/1. loc/base_seed/frame: the batch's
+// seed-advance tables (advance = false leaves them, e.g. for timing).
+// err: set to 1 when a row item's wait runs out.
+cudaError_t launch_persistent(const PersistItem* items, int nitems, uint32_t* ctl, int nworlds, int par,
+                              StepParams* const* loc, const uint32_t* base_seed, uint32_t* frame, bool advance,
+                              int* err, size_t smem, int grid, cudaStream_t s);
+
 // Column pass with its DFT stages on the tensor cores (lenia_fft_tc.cu), same
 // contract and layout as launch_col_fast: precision 1 = BF16 hi/lo, 2 = FP16
 // hi/lo operands (FP32 accumulation); H with an all-radix-16 plan (256, 4096);
