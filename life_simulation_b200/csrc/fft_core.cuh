@@ -29,11 +29,10 @@ __device__ __forceinline__ float2 csub(float2 a, float2 b) {
     return __ffma2_rn(b, make_float2(-1.0f, -1.0f), a);
 }
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
-    const float2 t = __fmul2_rn(make_float2(a.x, a.x), b);
-    return __ffma2_rn(make_float2(-a.y, a.y), make_float2(b.y, b.x), t);
+    return make_float2(__fmaf_rn(-a.y, b.y, __fmul_rn(a.x, b.x)), __fmaf_rn(a.y, b.x, __fmul_rn(a.x, b.y)));
 }
 __device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
-__device__ __forceinline__ float2 cscale(float2 a, float s) { return __fmul2_rn(a, make_float2(s, s)); }
+__device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(__fmul_rn(a.x, s), __fmul_rn(a.y, s)); }
 // -i*a (forward quarter turn) and +i*a.
 __device__ __forceinline__ float2 mul_mi(float2 a) { return make_float2(a.y, -a.x); }
 __device__ __forceinline__ float2 mul_pi(float2 a) { return make_float2(-a.y, a.x); }
@@ -64,7 +63,7 @@ template <bool INV>
 __device__ __forceinline__ void dft3(float2* v) {
     float2 t = cadd(v[1], v[2]);
     float2 d = csub(v[1], v[2]);
-    float2 m = __ffma2_rn(t, make_float2(kC3, kC3), v[0]);
+    float2 m = make_float2(__fmaf_rn(t.x, kC3, v[0].x), __fmaf_rn(t.y, kC3, v[0].y));
     v[0] = cadd(v[0], t);
     float2 r = rot90<INV>(cscale(d, kS3));  // -i*s*d forward
     v[1] = cadd(m, r);
@@ -87,12 +86,11 @@ __device__ __forceinline__ void dft5(float2* v) {
     float2 a2 = cadd(v[2], v[3]), b2 = csub(v[2], v[3]);
     float2 x0 = v[0];
     v[0] = cadd(x0, cadd(a1, a2));
-    const float2 C51 = make_float2(kC51, kC51), C52 = make_float2(kC52, kC52);
-    const float2 S51 = make_float2(kS51, kS51), S52 = make_float2(kS52, kS52);
-    float2 c1 = __ffma2_rn(a2, C52, __ffma2_rn(a1, C51, x0));
-    float2 c2 = __ffma2_rn(a2, C51, __ffma2_rn(a1, C52, x0));
-    float2 s1 = rot90<INV>(__ffma2_rn(b2, S52, __fmul2_rn(b1, S51)));
-    float2 s2 = rot90<INV>(__ffma2_rn(b2, make_float2(-kS51, -kS51), __fmul2_rn(b1, S52)));
+    const auto fma2 = [](float2 a, float k, float2 c) { return make_float2(__fmaf_rn(a.x, k, c.x), __fmaf_rn(a.y, k, c.y)); };
+    float2 c1 = fma2(a2, kC52, fma2(a1, kC51, x0));
+    float2 c2 = fma2(a2, kC51, fma2(a1, kC52, x0));
+    float2 s1 = rot90<INV>(fma2(b2, kS52, cscale(b1, kS51)));
+    float2 s2 = rot90<INV>(fma2(b2, -kS51, cscale(b1, kS52)));
     v[1] = cadd(c1, s1);
     v[4] = csub(c1, s1);
     v[2] = cadd(c2, s2);
@@ -102,17 +100,17 @@ __device__ __forceinline__ void dft5(float2* v) {
 // w_8^k for k = 1, 2, 3 applied to b (forward w = exp(-i*pi/4)).
 template <bool INV>
 __device__ __forceinline__ float2 w8_1(float2 b) {
-    // (b.x -/+ b.y, b.x +/- b.y) * sqrt(1/2)
-    const float2 s = INV ? __ffma2_rn(make_float2(b.y, b.y), make_float2(-1.0f, 1.0f), make_float2(b.x, b.x))
-                         : __ffma2_rn(make_float2(b.x, b.x), make_float2(1.0f, -1.0f), make_float2(b.y, b.y));
-    return __fmul2_rn(s, make_float2(kS2, kS2));
+    // forward: sqrt(1/2) * (b.x + b.y, b.y - b.x); inverse: sqrt(1/2) * (b.x - b.y, b.x + b.y)
+    const float2 s = INV ? make_float2(__fsub_rn(b.x, b.y), __fadd_rn(b.x, b.y))
+                         : make_float2(__fadd_rn(b.x, b.y), __fsub_rn(b.y, b.x));
+    return make_float2(__fmul_rn(s.x, kS2), __fmul_rn(s.y, kS2));
 }
 template <bool INV>
 __device__ __forceinline__ float2 w8_3(float2 b) {
     // forward: sqrt(1/2) * (b.y - b.x, -(b.x + b.y)); inverse: sqrt(1/2) * (-(b.x + b.y), b.x - b.y)
-    const float2 s = INV ? __ffma2_rn(make_float2(b.y, b.y), make_float2(-1.0f, -1.0f), make_float2(-b.x, b.x))
-                         : __ffma2_rn(make_float2(b.x, b.x), make_float2(-1.0f, -1.0f), make_float2(b.y, -b.y));
-    return __fmul2_rn(s, make_float2(kS2, kS2));
+    const float2 s = INV ? make_float2(-__fadd_rn(b.x, b.y), __fsub_rn(b.x, b.y))
+                         : make_float2(__fsub_rn(b.y, b.x), -__fadd_rn(b.x, b.y));
+    return make_float2(__fmul_rn(s.x, kS2), __fmul_rn(s.y, kS2));
 }
 
 template <bool INV>

@@ -83,8 +83,7 @@ __device__ __forceinline__ float2 twmul(float2 a) {
         return INV ? fft::mul_mi(a) : fft::mul_pi(a);
     } else {
         constexpr float wr = Tw<p, Q, INV>::re, wi = Tw<p, Q, INV>::im;
-        const float2 t = __fmul2_rn(make_float2(a.x, a.x), make_float2(wr, wi));
-        return __ffma2_rn(make_float2(a.y, a.y), make_float2(-wi, wr), t);
+        return make_float2(__fmaf_rn(a.y, -wi, __fmul_rn(a.x, wr)), __fmaf_rn(a.y, wr, __fmul_rn(a.x, wi)));
     }
 }
 

@@ -63,6 +63,54 @@ __device__ __forceinline__ void pass_gen(Src&& src, Dst&& dst, const float2* __r
     }
 }
 
+// The R outputs of one item of a first pass (span 1) are R consecutive
+// elements of a row: written two at a time (16-byte stores, half the store
+// instructions and shared-memory wavefronts) when R is even.
+// `row + base` must be 16-byte aligned when R is even (shared buffers at
+// even float2 offsets, even pitches, base a multiple of R).
+template <int R>
+__device__ __forceinline__ void store_run(float2* row, int base, const float2* v) {
+    if constexpr (R % 2 == 0) {
+        float4* d = reinterpret_cast<float4*>(row + base);
+#pragma unroll
+        for (int t = 0; t < R / 2; ++t) d[t] = make_float4(v[2 * t].x, v[2 * t].y, v[2 * t + 1].x, v[2 * t + 1].y);
+    } else {
+#pragma unroll
+        for (int t = 0; t < R; ++t) row[base + t] = v[t];
+    }
+}
+
+// Pass 0 (span 1) of plan P over a batch of B transforms into the shared
+// buffer `buf` (row pitch PITCH, even): pass_gen with store_run's stores.
+template <class P, bool INV, int B, int T, int PITCH, class Src>
+__device__ __forceinline__ void pass0_buf(Src&& src, float2* buf, int cols) {
+    using I = PassIdx<P, 0>;
+    static_assert(I::NS == 1, "the first pass has span 1");
+    constexpr int TOT = B * I::NR;
+    constexpr int ITEMS = (TOT + T - 1) / T;
+    float2 v[ITEMS][I::R];
+    int jj[ITEMS], bi[ITEMS];
+    bool ok[ITEMS];
+#pragma unroll
+    for (int it = 0; it < ITEMS; ++it) {
+        const int q = int(threadIdx.x) + it * T;
+        jj[it] = q / B;
+        bi[it] = q - jj[it] * B;
+        ok[it] = (TOT % T == 0 || q < TOT) && bi[it] < cols;
+        if (ok[it]) {
+#pragma unroll
+            for (int t = 0; t < I::R; ++t) v[it][t] = src(bi[it], I::in(jj[it], t));
+        }
+    }
+#pragma unroll
+    for (int it = 0; it < ITEMS; ++it) {
+        if (ok[it]) {
+            Dft<I::R, INV>::run(v[it]);
+            store_run<I::R>(buf + bi[it] * PITCH, jj[it] * I::R, v[it]);
+        }
+    }
+}
+
 // Passes PASS..LAST-1 between two shared buffers (barrier after each);
 // returns the buffer that holds the data afterwards.
 template <class P, int PASS, int LAST, bool INV, int B, int T, int PITCH>
@@ -105,9 +153,11 @@ struct ColK {
     static constexpr int T = roundup32((B * NRL + S - 1) / S);
     static constexpr int ITL = (B * NRL + T - 1) / T;
     static constexpr int PITCH = row_pitch(H);
-    static constexpr size_t smem() {
-        return sizeof(float2) * (size_t(PF::tw_size()) + PI::tw_size() + 2 * size_t(B) * PITCH + H);
-    }
+    // The work buffers start after the twiddle tables at an even float2
+    // offset (16-byte aligned, for store_run's paired stores).
+    static constexpr int BUF0 = (PF::tw_size() + PI::tw_size() + 1) / 2 * 2;
+    static_assert(PITCH % 2 == 0, "column pitch must keep 16-byte alignment");
+    static constexpr size_t smem() { return sizeof(float2) * (size_t(BUF0) + 2 * size_t(B) * PITCH + H); }
 };
 
 // Launch geometry of a row pass over RB rows per CTA iteration (inverse plan

@@ -253,7 +253,7 @@ __device__ __noinline__ void row_item(const SpectralWorld& sw, int y0, const flo
         bi[it] = q - jj[it] * RB;
         ok[it] = q < RB * NRC && bi[it] < rows;
     }
-    float acc[ITL][RC][2];
+    float2 acc[ITL][RC];  // growth sums of the pixel pair (2n, 2n + 1)
     for (int kk = 0; kk < nk; ++kk) {
         if (kk == 0) {
             cp_async_wait_prev();  // U_0's rows (A's may still be in flight)
@@ -270,7 +270,7 @@ __device__ __noinline__ void row_item(const SpectralWorld& sw, int y0, const flo
         const auto pick = [&](const float(&a)[kMaxKernels]) {
             return kk == 0 ? a[0] : kk == 1 ? a[1] : kk == 2 ? a[2] : a[3];
         };
-        const float mu = pick(p.mu), inv_sigma = 1.0f / pick(p.sigma), hw = pick(p.weight);
+        const GrowthPair gp(pick(p.mu), 1.0f / pick(p.sigma), pick(p.weight), asym);
 #pragma unroll
         for (int it = 0; it < ITL; ++it) {
             if (!ok[it]) continue;
@@ -282,15 +282,8 @@ __device__ __noinline__ void row_item(const SpectralWorld& sw, int y0, const flo
             const uint32_t gy = uint32_t(y0 + bi[it]);
 #pragma unroll
             for (int t = 0; t < RC; ++t) {
-                const uint32_t x0 = uint32_t(2 * (jj[it] + t * NRC));
-                const float m0 = jitter ? mu + mu_jitter_shift_call(p, x0, gy) : mu;
-                const float m1 = jitter ? mu + mu_jitter_shift_call(p, x0 + 1u, gy) : mu;
-                const float b0 = bell_fast(z[t].x, m0, inv_sigma);
-                const float b1 = bell_fast(z[t].y, m1, inv_sigma);
-                const float c0 = asym ? hw * b0 : hw * (2.0f * b0 - 1.0f);
-                const float c1 = asym ? hw * b1 : hw * (2.0f * b1 - 1.0f);
-                acc[it][t][0] = kk == 0 ? c0 : acc[it][t][0] + c0;
-                acc[it][t][1] = kk == 0 ? c1 : acc[it][t][1] + c1;
+                const float2 c = gp.term(z[t], p, jitter, uint32_t(2 * (jj[it] + t * NRC)), gy);
+                acc[it][t] = kk == 0 ? c : __fadd2_rn(acc[it][t], c);
             }
         }
         __syncthreads();  // sU and X read before sU is staged again
@@ -315,8 +308,8 @@ __device__ __noinline__ void row_item(const SpectralWorld& sw, int y0, const flo
                 const float A2 = asym ? A + dt * ((sw_ok ? s / sum_w : A) - A) : A + dt * s;
                 return fminf(fmaxf(A2, 0.0f), 1.0f);
             };
-            const float2 r = make_float2(finish(a.x, acc[it][t][0], uint32_t(2 * n)),
-                                         finish(a.y, acc[it][t][1], uint32_t(2 * n + 1)));
+            const float2 r = make_float2(finish(a.x, acc[it][t].x, uint32_t(2 * n)),
+                                         finish(a.y, acc[it][t].y, uint32_t(2 * n + 1)));
             *reinterpret_cast<float2*>(A_out + size_t(gy) * W + 2 * n) = r;
             za[it][t] = r;
         }

@@ -42,6 +42,36 @@ __device__ __forceinline__ float bell(float u, float mu, float sigma) {
 // relative error below 2^-22 (negligible against the FP32 FFT's rounding),
 // and it replaces an IEEE division and the full-range expf sequence; used on
 // the spectral path, where the growth map is a large share of the row pass.
+// 2^x by the SFU's approximate base-2 exponential (relative error < 2^-22,
+// subnormal results flushed to zero).
+__device__ __forceinline__ float ex2_fast(float x) {
+    float r;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+// One kernel's growth terms at a pixel pair of the spectral row passes:
+// bell(u) = exp(-(u - mu)^2 / (2 sigma^2)) = 2^-((u*sc - mu*sc)^2) with
+// sc = sqrt(log2(e) / 2) / sigma, and the term h * (2 bell - 1) (growth mode
+// 0) or h * bell (mode 1) as g1 * bell + g0 -- in packed FP32x2 pairs (one
+// FFMA2, one FMUL2, two SFU exponentials, one FFMA2 per pair). With mu
+// jitter the pair's centres come per pixel (mu + shift).
+struct GrowthPair {
+    float mu, sc;
+    float2 SC, MSC, G1, G0;
+    __device__ __forceinline__ GrowthPair(float mu_, float inv_sigma, float h, bool asym) : mu(mu_) {
+        sc = inv_sigma * 0.84932180028801904272f;
+        SC = make_float2(sc, sc);
+        MSC = make_float2(-mu * sc, -mu * sc);
+        const float g1 = asym ? h : 2.0f * h, g0 = asym ? 0.0f : -h;
+        G1 = make_float2(g1, g1);
+        G0 = make_float2(g0, g0);
+    }
+    // u: the potentials of pixels (x0, gy), (x0 + 1, gy).
+    __device__ __forceinline__ float2 term(float2 u, const StepParams& p, bool jitter, uint32_t x0,
+                                           uint32_t gy) const;
+};
+
 __device__ __forceinline__ float bell_fast(float u, float mu, float inv_sigma) {
     const float t = (u - mu) * inv_sigma;
     float r;
@@ -109,6 +139,21 @@ static __device__ __noinline__ float growth_finish_call(const StepParams& p, flo
 }
 static __device__ __noinline__ float mu_jitter_shift_call(const StepParams& p, uint32_t gx, uint32_t gy) {
     return mu_jitter_shift(p, gx, gy);
+}
+
+__device__ __forceinline__ float2 GrowthPair::term(float2 u, const StepParams& p, bool jitter, uint32_t x0,
+                                                   uint32_t gy) const {
+    float2 d;  // (u - mu) * sc for both pixels
+    if (jitter) {
+        const float m0 = mu + mu_jitter_shift_call(p, x0, gy);
+        const float m1 = mu + mu_jitter_shift_call(p, x0 + 1u, gy);
+        d = make_float2((u.x - m0) * sc, (u.y - m1) * sc);
+    } else {
+        d = __ffma2_rn(u, SC, MSC);
+    }
+    const float2 q = __fmul2_rn(d, d);
+    const float2 b = make_float2(ex2_fast(-q.x), ex2_fast(-q.y));
+    return __ffma2_rn(b, G1, G0);
 }
 // growth_finish with the common case (no noise, no injection) inline.
 __device__ __forceinline__ float growth_finish_lean(const StepParams& p, float A, float weighted, float std_sum,

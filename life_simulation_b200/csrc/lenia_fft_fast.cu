@@ -58,8 +58,7 @@ using namespace fastfft;
 template <class PF, int B, int S = 1>
 struct ColStage {
     using K = ColK<PF, B, S>;
-    static constexpr int OFF =
-        (PF::tw_size() + K::PI::tw_size() + 2 * B * K::PITCH + K::H + 1) / 2 * 2;  // 16-byte aligned
+    static constexpr int OFF = (K::BUF0 + 2 * B * K::PITCH + K::H + 1) / 2 * 2;  // 16-byte aligned
     static constexpr size_t with_stage = sizeof(float2) * (size_t(OFF) + size_t(B) * K::H);
     // Not with S = 2, whose CTAs are meant to fit two per SM.
     static constexpr bool on = S == 1 && B % 2 == 0 && with_stage <= 227 * 1024;
@@ -78,7 +77,7 @@ __global__ void __launch_bounds__(ColK<PF, B, SPLIT>::T)
     __shared__ SpectralWorld sw;  // this CTA's world
     float2* twf = sm;
     float2* twi = twf + PF::tw_size();
-    float2* ba = twi + PI::tw_size();
+    float2* ba = sm + K::BUF0;
     float2* bb = ba + B * PITCH;
     float2* c0 = bb + B * PITCH;
     copy_table(twf, twf_g, PF::tw_size());
@@ -146,14 +145,13 @@ __global__ void __launch_bounds__(ColK<PF, B, SPLIT>::T)
         if constexpr (CS::on) {
             cp_async_wait_all();
             __syncthreads();  // this group's rows staged
-            pass_gen<PF, 0, false, B, T>([&](int b, int i) { return bs[i * B + b]; },
-                                          [&](int b, int i, float2 v) { ba[b * PITCH + i] = v; }, twf, cols);
+            pass0_buf<PF, false, B, T, PITCH>([&](int b, int i) { return bs[i * B + b]; }, ba, cols);
             __syncthreads();  // bs read: the next group's rows may land
             const int next = k0 + int(gridDim.x) * B;
             if (next < M) stage_group(next);
         } else {
-            pass_gen<PF, 0, false, B, T>([&](int b, int i) { return __ldg(S + gbase + size_t(i) * KB + b); },
-                                          [&](int b, int i, float2 v) { ba[b * PITCH + i] = v; }, twf, cols);
+            pass0_buf<PF, false, B, T, PITCH>([&](int b, int i) { return __ldg(S + gbase + size_t(i) * KB + b); }, ba,
+                                              cols);
             __syncthreads();
         }
         float2* X = mid_passes<PF, 1, PF::np - 1, false, B, T, PITCH>(ba, bb, twf, cols);
@@ -209,8 +207,7 @@ __global__ void __launch_bounds__(ColK<PF, B, SPLIT>::T)
                     }
                 }
                 Dft<RL, true>::run(D);
-#pragma unroll
-                for (int t = 0; t < RL; ++t) Y[bi[it] * PITCH + jj[it] * RL + t] = D[t];
+                store_run<RL>(Y + bi[it] * PITCH, jj[it] * RL, D);
             }
             if (kk + 1 < nk) fetch_k(kk + 1);
         };
@@ -338,7 +335,7 @@ __global__ void __launch_bounds__(RowK<PI, RB, SPLIT>::T,
             bi[it] = q - jj[it] * RB;
             ok[it] = q < RB * NRC && bi[it] < rows;
         }
-        float acc[K::ITL][RC][2];
+        float2 acc[K::ITL][RC];  // growth sums of the pixel pair (2n, 2n + 1)
         for (int kk = 0; kk < nk; ++kk) {
             float2* cur = stg(base + kk);
             if constexpr (PIPE) {
@@ -356,8 +353,8 @@ __global__ void __launch_bounds__(RowK<PI, RB, SPLIT>::T,
                 __syncthreads();
             }
             // Inverse of the real-FFT split folded into the first pass's loads.
-            pass_gen<PI, 0, true, RB, T>([&](int b, int i) { return c2r_split<M>(cur + b * PITCH, twr, i); },
-                                         [&](int b, int i, float2 v) { bw[b * PITCH + i] = v; }, twi, rows);
+            pass0_buf<PI, true, RB, T, PITCH>([&](int b, int i) { return c2r_split<M>(cur + b * PITCH, twr, i); }, bw,
+                                              rows);
             __syncthreads();
             float2* X = mid_passes<PI, 1, PI::np - 1, true, RB, T, PITCH>(bw, cur, twi, rows);
             // Selects instead of a dynamic index into the parameter block (which
@@ -365,7 +362,7 @@ __global__ void __launch_bounds__(RowK<PI, RB, SPLIT>::T,
             const auto pick = [&](const float(&a)[kMaxKernels]) {
                 return kk == 0 ? a[0] : kk == 1 ? a[1] : kk == 2 ? a[2] : a[3];
             };
-            const float mu = pick(p.mu), inv_sigma = 1.0f / pick(p.sigma), hw = pick(p.weight);
+            const GrowthPair gp(pick(p.mu), 1.0f / pick(p.sigma), pick(p.weight), asym);
             // Last inverse pass into registers: u[2n], u[2n+1] for n = j + t*NRC.
 #pragma unroll
             for (int it = 0; it < K::ITL; ++it) {
@@ -383,15 +380,8 @@ __global__ void __launch_bounds__(RowK<PI, RB, SPLIT>::T,
                 }
 #pragma unroll
                 for (int t = 0; t < RC; ++t) {
-                    const uint32_t x0 = uint32_t(2 * (jj[it] + t * NRC));
-                    const float m0 = jitter ? mu + mu_jitter_shift_call(p, x0, gy) : mu;
-                    const float m1 = jitter ? mu + mu_jitter_shift_call(p, x0 + 1u, gy) : mu;
-                    const float b0 = bell_fast(z[t].x, m0, inv_sigma);
-                    const float b1 = bell_fast(z[t].y, m1, inv_sigma);
-                    const float c0 = asym ? hw * b0 : hw * (2.0f * b0 - 1.0f);
-                    const float c1 = asym ? hw * b1 : hw * (2.0f * b1 - 1.0f);
-                    acc[it][t][0] = kk == 0 ? c0 : acc[it][t][0] + c0;
-                    acc[it][t][1] = kk == 0 ? c1 : acc[it][t][1] + c1;
+                    const float2 c = gp.term(z[t], p, jitter, uint32_t(2 * (jj[it] + t * NRC)), gy);
+                    acc[it][t] = kk == 0 ? c : __fadd2_rn(acc[it][t], c);
                 }
             }
             if constexpr (!PIPE) __syncthreads();  // cur (the one staging buffer) read
@@ -431,8 +421,8 @@ __global__ void __launch_bounds__(RowK<PI, RB, SPLIT>::T,
                     const float A2 = asym ? A + dt * ((sw_ok ? s / sum_w : A) - A) : A + dt * s;
                     return fminf(fmaxf(A2, 0.0f), 1.0f);
                 };
-                const float2 r = make_float2(finish(a.x, acc[it][t][0], uint32_t(2 * n)),
-                                             finish(a.y, acc[it][t][1], uint32_t(2 * n + 1)));
+                const float2 r = make_float2(finish(a.x, acc[it][t].x, uint32_t(2 * n)),
+                                             finish(a.y, acc[it][t].y, uint32_t(2 * n + 1)));
                 *reinterpret_cast<float2*>(A_out + size_t(gy) * W + 2 * n) = r;
                 if constexpr (CM) palette_pair(sw.cm, r, sw.rgba + size_t(gy) * W + 2 * n);
                 za[it][t] = r;
@@ -447,8 +437,7 @@ __global__ void __launch_bounds__(RowK<PI, RB, SPLIT>::T,
         for (int it = 0; it < K::ITL; ++it) {
             if (!ok[it]) continue;
             Dft<RC, false>::run(za[it]);
-#pragma unroll
-            for (int t = 0; t < RC; ++t) bw[bi[it] * PITCH + jj[it] * RC + t] = za[it][t];
+            store_run<RC>(bw + bi[it] * PITCH, jj[it] * RC, za[it]);
         }
         __syncthreads();
         float2* Y = mid_passes<PF, 1, PF::np - 1, false, RB, T, PITCH>(bw, sA, twf, rows);
