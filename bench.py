@@ -112,6 +112,11 @@ def parse_args():
     ap.add_argument("--no-library-baseline", action="store_true")
     ap.add_argument("--no-sweep", action="store_true", help="skip the 512-world sweep in the step line")
     ap.add_argument("--no-tc", action="store_true", help="skip the 4096^2 tensor-core comparison in the step line")
+    ap.add_argument("--tc-variants", default=None,
+                    help="--mode tc: comma-separated subset of fp32, fp16x3, bf16x3, fp16x3_tcgen05, bf16x3_tcgen05, "
+                         "fp16x3_tcgen05_pipelined, bf16x3_tcgen05_pipelined")
+    ap.add_argument("--tc-steps", type=int, default=64, help="--mode tc: timed steps per variant")
+    ap.add_argument("--no-tc-error", action="store_true", help="--mode tc: skip the FP64 error check")
     ap.add_argument("--launch-shape", default=None,
                     help="columns,rows per CTA of the two passes, e.g. 4,4p (p: pipelined rows; "
                          "h after the columns: half-thread column pass); "
@@ -884,7 +889,7 @@ def run_adjoint(args):
     return 0
 
 
-def tc_bench(warmup: int = 3, steps: int = 64, error_check: bool = True) -> dict:
+def tc_bench(warmup: int = 3, steps: int = 64, error_check: bool = True, only=None) -> dict:
     """4096x4096, 3 kernels R=32: the column DFT stages on the CUDA cores (FP32)
     and on the tensor cores (FP16 / BF16 hi/lo, FP32 accumulation): per
     precision the device time per step, the column pass's HBM roofline and
@@ -903,15 +908,35 @@ def tc_bench(warmup: int = 3, steps: int = 64, error_check: bool = True) -> dict
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     peak, peak_kind = measured_peaks()
     col_bytes = (4 + 2 * K + 4 * K) * w * h
-    # (1 forward + K inverse) column transforms x 3 radix-16 stages x H points
-    # x 128 FLOP (real 32x32 GEMM per 16 points) x 3 (hi/lo), per column.
-    tc_flops = (1 + K) * 3 * h * 128 * 3 * (w // 2)
+    # Tensor FLOPs per column launch, (1 forward + K inverse) transforms per
+    # column: mma.sync engine, 3 radix-16 stages x H points x 128 FLOP (real
+    # 32x32 GEMM per 16 points) x 3 (hi/lo); tcgen05 engine, 2 radix-64
+    # passes x H/64 items x 2 x 128 x 128 x 3 (real 128x128 GEMM per 64
+    # points, hi/lo).
+    tc05_flops = (1 + K) * 2 * (h // 64) * 2 * 128 * 128 * 3 * (w // 2)
+    tc_flops = {"mma": (1 + K) * 3 * h * 128 * 3 * (w // 2), "tcgen05_serial": tc05_flops,
+                "tcgen05_pipelined": tc05_flops}
     res = {}
-    for prec in ("fp32", "fp16x3", "bf16x3"):
+    variants = (("fp32", "fp32", None), ("fp16x3", "fp16x3", "mma"), ("bf16x3", "bf16x3", "mma"),
+                ("fp16x3_tcgen05", "fp16x3", "tcgen05_serial"), ("bf16x3_tcgen05", "bf16x3", "tcgen05_serial"),
+                ("fp16x3_tcgen05_pipelined", "fp16x3", "tcgen05_pipelined"),
+                ("bf16x3_tcgen05_pipelined", "bf16x3", "tcgen05_pipelined"))
+    for name, prec, engine in variants:
+        if only and name not in only:
+            continue
         p = wl.fft3_params(w, h)
         p["radius"] = 32
         p["fftPrecision"] = prec
-        m = lb.LeniaModule(p, w, h)
+        # LENIA_TC_ENGINE at setup keeps one engine's candidates.
+        old_engine = os.environ.pop("LENIA_TC_ENGINE", None)
+        if engine:
+            os.environ["LENIA_TC_ENGINE"] = engine
+        try:
+            m = lb.LeniaModule(p, w, h)
+        finally:
+            os.environ.pop("LENIA_TC_ENGINE", None)
+            if old_engine is not None:
+                os.environ["LENIA_TC_ENGINE"] = old_engine
         m.reset(2)
         m.upload(init)
         fp = m.frame_params(0)
@@ -937,9 +962,9 @@ def tc_bench(warmup: int = 3, steps: int = 64, error_check: bool = True) -> dict
         r = {"ms_per_step": step_ms, "mpx_steps_s": w * h / (step_ms / 1e3) / 1e6,
              "column_ms": col_ms, "row_ms": prof["row_growth"]["ms"] / prof["row_growth"]["count"],
              "column_gbs": col_bytes / (col_ms / 1e3) / 1e9, "column_frac_hbm": col_bytes / (col_ms / 1e3) / 1e9 / peak,
-             "fft_precision": m.info()["fft_precision"]}
+             "fft_precision": m.info()["fft_precision"], "tc_engine": m.info()["tc_engine"]}
         if prec != "fp32":
-            r["column_tensor_tflops"] = tc_flops / (col_ms / 1e3) / 1e12
+            r["column_tensor_tflops"] = tc_flops[engine] / (col_ms / 1e3) / 1e12
         if error_check:
             # One step from the seeded field itself (alive; the timed steps
             # have let the patches decay by now).
@@ -948,7 +973,7 @@ def tc_bench(warmup: int = 3, steps: int = 64, error_check: bool = True) -> dict
             m.step(fp, 1, sh)
             torch.cuda.synchronize()
             r["_next"] = m.field()
-        res[prec] = r
+        res[name] = r
         m.close()
     if error_check:
         from oracle import lenia_oracle as lo
@@ -967,6 +992,9 @@ def tc_bench(warmup: int = 3, steps: int = 64, error_check: bool = True) -> dict
     return {"workload": "4096x4096, 3 kernels R=32 (fft3 peaks/mu/sigma/h), 40 patches of 256x256 (seed 2)",
             "steps": steps, "l2": "256 MiB write between steps", "peak_hbm_gbs": peak, "peak_source": peak_kind,
             "column_bytes_per_launch": col_bytes, "column_tensor_flops_per_launch": tc_flops,
+            "engines": "tc_engine 1: mma.sync radix-16 tiles; 2: tcgen05 radix-64 GEMMs, accumulators in tensor "
+                       "memory, each pass waited for; 3: the same over two operand slots, one kernel's MMAs "
+                       "overlapping the next kernel's operand build",
             "error": "one step from the seeded field vs one FP64 oracle step from it",
             "precisions": res}
 
@@ -975,10 +1003,13 @@ def run_tc(args):
     import torch
 
     torch.cuda.set_device(0)
-    r = tc_bench(args.warmup)
+    only = set(args.tc_variants.split(",")) if args.tc_variants else None
+    r = tc_bench(args.warmup, args.tc_steps, not args.no_tc_error, only)
+    first = next(iter(r["precisions"].values()))
     line = {"metric": "Lenia Mpixel-steps/s, 4096x4096 K=3 R=32: column DFT stages FP32 CUDA cores vs "
                       "split-precision tensor cores",
-            "unit": UNIT, "value": r["precisions"]["fp32"]["mpx_steps_s"], "higher_is_better": True, "n_gpus": 1,
+            "unit": UNIT, "value": r["precisions"].get("fp32", first)["mpx_steps_s"], "higher_is_better": True,
+            "n_gpus": 1,
             "dtype": "f32 / fp16x3 / bf16x3", "data": "synthetic", "config": {"workload": r["workload"]}}
     line.update(r)
     print(json.dumps(line))

@@ -132,6 +132,9 @@ typedef struct lenia_info {
     uint32_t direct_outputs_per_thread; /* direct path: 8, or 16 on large tiles where faster */
     uint32_t direct_taps;     /* direct path: nonzero kernel taps summed over its kernels */
     uint32_t direct_rows_per_thread; /* direct path: output rows per thread, 1 or 2 (large tiles where faster) */
+    uint32_t tc_engine;       /* column DFT stages on the tensor cores: 0 none, 1 mma.sync tiles (radix 16),
+                                 2 tcgen05 GEMMs (radix 64, 4096-row fields), 3 the same pipelined over
+                                 two operand slots */
 } lenia_info;
 
 typedef struct lenia_ctx lenia_ctx;

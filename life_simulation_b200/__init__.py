@@ -84,7 +84,7 @@ class Info(ctypes.Structure):
                 ("fft_radix_col", ctypes.c_uint32 * 8), ("fft_precision", ctypes.c_uint32),
                 ("direct_tma", ctypes.c_uint32), ("direct_split", ctypes.c_uint32),
                 ("direct_outputs_per_thread", ctypes.c_uint32), ("direct_taps", ctypes.c_uint32),
-                ("direct_rows_per_thread", ctypes.c_uint32)]
+                ("direct_rows_per_thread", ctypes.c_uint32), ("tc_engine", ctypes.c_uint32)]
 
 
 # Every symbol include/lenia_b200.h declares (checked by the CPU tests).
@@ -501,7 +501,7 @@ class LeniaModule:
                 "fft_radix_col": [r for r in i.fft_radix_col if r], "fft_precision": i.fft_precision,
                 "direct_tma": bool(i.direct_tma), "direct_split": i.direct_split,
                 "direct_outputs_per_thread": i.direct_outputs_per_thread, "direct_taps": i.direct_taps,
-                "direct_rows_per_thread": i.direct_rows_per_thread}
+                "direct_rows_per_thread": i.direct_rows_per_thread, "tc_engine": i.tc_engine}
 
 
 def inspect(params, scene_w: int, scene_h: int, base_dir: Optional[str] = None) -> dict:

@@ -227,6 +227,19 @@ cudaError_t launch_persistent(const PersistItem* items, int nitems, uint32_t* ct
 bool tc_col_plan(int H);
 cudaError_t launch_col_tc(const FftGeometry& g, const FastTables& t, int precision, int batch, const float2* S,
                           float2* U, cudaStream_t s);
+// The same column pass for H = 4096 with its DFT stages as tcgen05 GEMMs
+// (lenia_fft_tc05.cu: two radix-64 passes, operands in shared memory,
+// accumulators in tensor memory); same precisions and contract. pipelined:
+// two operand slots, so one kernel's MMAs overlap the next kernel's operand
+// build. err: device counter of CTAs whose wait for an MMA ran out (or null).
+bool tc05_col_plan(int H);
+cudaError_t launch_col_tc05(const FftGeometry& g, int precision, bool pipelined, const float2* S, float2* U,
+                            int* err, cudaStream_t s);
+// Column-pass choices of a context whose column stages run on the tensor
+// cores, beside the mma.sync pass's columns-per-CTA counts: the tcgen05 pass,
+// serial or pipelined.
+constexpr int kTcgen05 = 0x80;
+constexpr int kTcgen05Pipelined = 0x81;
 
 // Colour map (lenia_colormap.cu): the field (w x h) to ow x oh RGBA16F
 // (ushort4 per pixel); bilinear with wrapping when the sizes differ.

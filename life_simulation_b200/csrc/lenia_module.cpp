@@ -905,6 +905,12 @@ int LeniaModule::buildDirectTables() {
     return LENIA_OK;
 }
 
+cudaError_t LeniaModule::launchColumnTc(int choice, const float2* S, float2* U, cudaStream_t s) {
+    if (choice == kTcgen05 || choice == kTcgen05Pipelined)
+        return launch_col_tc05(fgeo_, int(tc_precision_), choice == kTcgen05Pipelined, S, U, d_tma_err_, s);
+    return launch_col_tc(fgeo_, fast_, int(tc_precision_), choice, S, U, s);
+}
+
 int LeniaModule::checkDeviceFlags() {
     if (!d_tma_err_) return LENIA_OK;
     int n = 0;
@@ -912,6 +918,10 @@ int LeniaModule::checkDeviceFlags() {
     if (e != cudaSuccess) return cudaFail(e, "read device flags");
     if (n != 0) {
         cudaMemset(d_tma_err_, 0, sizeof(int));
+        if (use_fft_)
+            return fail(LENIA_ERR_CUDA, "tensor-core column pass: " + std::to_string(n) +
+                                            " CTA(s) stopped after a wait for an MMA ran out; their columns were "
+                                            "not written");
         return fail(LENIA_ERR_CUDA, "direct path: " + std::to_string(n) +
                                         " halo tile load(s) did not arrive in time; those tiles were not written");
     }
@@ -1003,6 +1013,12 @@ int LeniaModule::buildSpectralTables(const std::vector<KernelDef>& eff) {
         fast_.row_twi = d_fast_tw_[2];
         fast_.row_twf = d_fast_tw_[3];
     }
+    if (tc_precision_ != LENIA_FFT_FP32 && tc05_col_plan(int(h_)) && !d_tma_err_) {
+        // The tcgen05 column pass counts CTAs whose MMA wait ran out here.
+        cudaError_t e;
+        if ((e = dev_alloc(&d_tma_err_, 1, device_bytes_)) != cudaSuccess) return cudaFail(e, "cudaMalloc flags");
+        cudaMemset(d_tma_err_, 0, sizeof(int));
+    }
     return autotuneSpectral();
 }
 
@@ -1062,12 +1078,25 @@ int LeniaModule::autotuneSpectral() {
         if (t < 0.97f * best_row) { best_row = t; row_batch_ = c; }
     }
     if (tc_precision_ != LENIA_FFT_FP32) {
+        // Candidates: the tcgen05 pass (4096-row fields) and the mma.sync
+        // pass at each columns-per-CTA count. LENIA_TC_ENGINE=tcgen05 or
+        // =mma at setup keeps only that engine's candidates.
+        const char* eng = std::getenv("LENIA_TC_ENGINE");
+        const std::string e = eng ? eng : "";
+        std::vector<int> cands;
+        if (tc05_col_plan(int(h_))) {
+            if (e.empty() || e == "tcgen05" || e == "tcgen05_pipelined") cands.push_back(kTcgen05Pipelined);
+            if (e.empty() || e == "tcgen05" || e == "tcgen05_serial") cands.push_back(kTcgen05);
+        }
+        if (cands.empty() || e.empty() || e == "mma")
+            for (int c : {8, 4, 2, 1}) cands.push_back(c);
         float best_tc = 1e30f;
-        for (int c : {8, 4, 2, 1}) {
-            const float t = time_it([&] { return launch_col_tc(fgeo_, fast_, int(tc_precision_), c, d_S_, d_U_, stream_); });
+        for (int c : cands) {
+            const float t = time_it([&] { return launchColumnTc(c, d_S_, d_U_, stream_); });
             if (t < 0.97f * best_tc) { best_tc = t; tc_batch_ = c; }
         }
         if (best_tc >= 1e29f) tc_precision_ = LENIA_FFT_FP32;
+        cudaGetLastError();
     }
     if (best_col >= 1e29f || best_row >= 1e29f) fast_col_ = fast_row_ = false;
     cudaGetLastError();
@@ -1311,8 +1340,7 @@ int LeniaModule::stepImpl(const lenia_frame_params& fp, uint32_t substeps, cudaS
                 if (e != cudaSuccess) return cudaFail(e, "row pass");
             }
             e = launch(LENIA_PHASE_COLUMN, s, [&] {
-                if (tc_precision_ != LENIA_FFT_FP32)
-                    return launch_col_tc(fgeo_, fast_, int(tc_precision_), tc_batch_, d_S_, d_U_, s);
+                if (tc_precision_ != LENIA_FFT_FP32) return launchColumnTc(tc_batch_, d_S_, d_U_, s);
                 return fast_col_ ? launch_col_fast(fgeo_, fast_, col_batch_, d_S_, d_U_, s)
                                  : launch_col_conv(fgeo_, d_S_, d_U_, s);
             });
@@ -1347,6 +1375,10 @@ void LeniaModule::info(lenia_info* o) const {
     o->use_stamp_init = use_stamp_ ? 1u : 0u;
     o->device_bytes = device_bytes_;
     o->fft_precision = tc_precision_;
+    o->tc_engine = tc_precision_ == LENIA_FFT_FP32 ? 0u
+                   : tc_batch_ == kTcgen05          ? 2u
+                   : tc_batch_ == kTcgen05Pipelined ? 3u
+                                                    : 1u;
     o->direct_tma = (!use_fft_ && direct_tma_.on) ? 1u : 0u;
     o->direct_split = use_fft_ ? 0u : uint32_t(direct_split_);
     o->direct_outputs_per_thread = use_fft_ ? 0u : uint32_t(direct_ox_);

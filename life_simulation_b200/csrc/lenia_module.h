@@ -151,6 +151,8 @@ private:
     int buildDirectTables();
     int buildSpectralTables(const std::vector<KernelDef>& eff);
     int autotuneSpectral();
+    // The tensor-core column pass: kTcgen05, or mma.sync at `choice` columns per CTA.
+    cudaError_t launchColumnTc(int choice, const float2* S, float2* U, cudaStream_t s);
     int stepImpl(const lenia_frame_params& fp, uint32_t substeps, cudaStream_t stream, void* rgba16f);
     int initField(const lenia_frame_params& fp, cudaStream_t s);
     int initKernels(const lenia_frame_params& fp);
@@ -190,7 +192,7 @@ private:
     // Device resources.
     float* field_[2] = {nullptr, nullptr};
     DirectTma direct_tma_;          // halo-tile tensor maps of field_[0], field_[1]
-    int* d_tma_err_ = nullptr;      // halo loads whose wait ran out
+    int* d_tma_err_ = nullptr;      // halo loads (direct) or MMA waits (tcgen05 column pass) that ran out
     float* d_weights_ = nullptr;
     uint32_t* d_spans_ = nullptr;
     float* d_org_ = nullptr;

@@ -83,3 +83,91 @@ def test_tensor_core_size_fallback():
     m = lb.LeniaModule(tc_params(512, 256, "fp64"), 512, 256)
     assert "fftPrecision" in m.warning and m.info()["fft_precision"] == lb.FFT_FP32
     m.close()
+
+
+def tc_module(params, w, h, engine):
+    """A module whose setup keeps only `engine`'s tensor-core candidates
+    (LENIA_TC_ENGINE, read at setup)."""
+    import os
+
+    old = os.environ.get("LENIA_TC_ENGINE")
+    os.environ["LENIA_TC_ENGINE"] = engine
+    try:
+        return lb.LeniaModule(params, w, h)
+    finally:
+        if old is None:
+            os.environ.pop("LENIA_TC_ENGINE", None)
+        else:
+            os.environ["LENIA_TC_ENGINE"] = old
+
+
+TC05_ENGINE = {"tcgen05_serial": 2, "tcgen05_pipelined": 3}
+
+
+@pytest.mark.parametrize("engine", ["tcgen05_serial", "tcgen05_pipelined"])
+def test_tcgen05_engine_4096_per_step_vs_fp64(engine):
+    """The tcgen05 column pass (radix-64 GEMMs, accumulators in tensor
+    memory; each pass waited for, or two operand slots in flight) at
+    4096x4096, 3 kernels R=32: per-step error against FP64 under the same
+    bounds as the mma.sync engine."""
+    import os
+
+    w = h = 4096
+    init = wl.patches(w, h, 40, 256, seed=2)
+    for prec in ("fp16x3", "bf16x3"):
+        params = tc_params(w, h, prec, radius=32)
+        m = tc_module(params, w, h, engine)
+        info = m.info()
+        assert info["tc_engine"] == TC05_ENGINE[engine] and info["fft_precision"] == PREC[prec], info
+        m.close()
+        os.environ["LENIA_TC_ENGINE"] = engine
+        try:
+            errs = step_errors(params, w, h, init, 2)
+        finally:
+            os.environ.pop("LENIA_TC_ENGINE", None)
+        print(f"4096x4096 {prec} {engine}: per-step max {errs[:, 0].max():.2e} RMS {errs[:, 1].max():.2e}")
+        assert errs[:, 0].max() <= TOL[prec], (prec, errs)
+
+
+def test_tcgen05_forms_give_the_same_bits():
+    """Serial and pipelined tcgen05 passes issue the same MMAs on the same
+    operands: the same field after three steps."""
+    w = h = 4096
+    init = wl.patches(w, h, 40, 256, seed=3)
+    out = []
+    for engine in ("tcgen05_serial", "tcgen05_pipelined"):
+        m = tc_module(tc_params(w, h, "fp16x3", radius=32), w, h, engine)
+        m.reset(3)
+        m.upload(init)
+        fp = m.frame_params(0)
+        for s in range(3):
+            fp.frame_index = fp.audio_frame = s
+            m.step(fp, 1)
+        out.append(m.field())
+        m.close()
+    np.testing.assert_array_equal(out[0], out[1])
+
+
+def test_tcgen05_engine_equals_fp32_path_closely():
+    """Ten chained steps: the tcgen05 engine's field stays within 1e-3 of
+    the FP32 CUDA-core path's (per-step differences of ~1e-5 compound through
+    the growth bells), and lenia_sync reports no MMA wait that ran out."""
+    w = h = 4096
+    init = wl.patches(w, h, 40, 256, seed=5)
+    fields = {}
+    for prec, engine in (("fp32", None), ("fp16x3", "tcgen05")):
+        params = tc_params(w, h, prec, radius=32)
+        m = tc_module(params, w, h, engine) if engine else lb.LeniaModule(params, w, h)
+        if engine:
+            assert m.info()["tc_engine"] in (2, 3)
+        m.reset(3)
+        m.upload(init)
+        fp = m.frame_params(0)
+        for s in range(10):
+            fp.frame_index = fp.audio_frame = s
+            m.step(fp, 1)
+        m.sync()
+        fields[prec] = m.field()
+        m.close()
+    d = np.abs(fields["fp16x3"] - fields["fp32"]).max()
+    assert d <= 1e-3, d
