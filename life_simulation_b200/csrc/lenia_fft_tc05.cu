@@ -8,7 +8,8 @@
 // column FFT of FFT_H(S) * khat_k.
 //
 // 4096 = 64 x 64: two radix-64 Stockham passes per transform. One pass over
-// B = 2 columns is one GEMM: 128 items (64 per column) of 64 complex inputs,
+// B = 2 columns is one GEMM: 128 items (64 per column, the two columns'
+// items interleaved: GEMM item 2j + b is item j of column b) of 64 complex inputs,
 // i.e. in real arithmetic a 128 x 128 operand X (K = 128: re/im of the 64
 // inputs interleaved) against the 128 x 128 real DFT matrix
 //     F[2u + c][2t + c'] = ([[cos, sin], [-sin, cos]] of 2 pi u t / 64) / 64
@@ -31,6 +32,9 @@
 // IDFT(x) = conj(DFT(conj(x))), and with conjugated data the inverse
 // twiddles become the forward ones: one DFT matrix and one twiddle rule
 // serve both directions.
+//
+// Sixteen warps: warp w reads tensor-memory lanes 32 (w % 4) .. + 31 and
+// columns kCW (w / 4) .. + kCW - 1 of every result.
 //
 // Tensor memory: 256 columns per CTA, [0, 128) the current pass's result,
 // [128, 256) the forward column spectrum, kept for all kernels' products
@@ -57,11 +61,12 @@ using namespace fastfft;
 constexpr int kH = 4096;                     // column length
 constexpr int kHh = kH / 2 + 1;              // kernel spectrum rows
 constexpr int kB = 2;                        // columns per group
-constexpr int kT = 256;                      // 8 warps: two per tensor-memory lane quadrant
+constexpr int kT = 512;                      // 16 warps: four per tensor-memory lane quadrant
+constexpr int kCW = 128 / (kT / 128);        // tensor-memory columns per warp (32)
 constexpr uint32_t kTmemCols = 256;
 constexpr uint32_t kOp = 128u * 128u * 2u;   // one 128 x 128 16-bit operand (32 KB)
 // Dynamic shared memory: F hi/lo, operand slot 0 hi/lo, (pipelined: slot 1
-// hi/lo,) the 4096 roots of unity.
+// hi/lo,) the second pass's 4096 twiddles.
 constexpr uint32_t kSmFhi = 0, kSmFlo = kOp, kSmXhi = 2 * kOp, kSmXlo = 3 * kOp, kSmRoot = 4 * kOp;
 constexpr size_t kSmem = 4 * size_t(kOp) + size_t(kH) * sizeof(float2);  // 160 KB (224 KB pipelined)
 constexpr float kProductScale = 16777216.0f;  // 2^24 = 4096^2: the two 1/64 of each transform's passes
@@ -137,49 +142,23 @@ __device__ __forceinline__ void issue_pass(uint32_t d, uint32_t a_hi, uint32_t a
                  : "memory");
 }
 
-// All threads: make the operand writes visible to the tensor cores, run one
-// pass and wait for it (bounded). False (for every thread) if the wait ran out.
-template <int PREC>
-__device__ __forceinline__ bool run_pass(uint32_t d, uint32_t a_hi, uint32_t a_lo, uint32_t b_hi, uint32_t b_lo,
-                                         uint64_t* bar, uint32_t& phase) {
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        issue_pass<PREC>(d, a_hi, a_lo, b_hi, b_lo, bar);
-    }
-    const bool done = mbar_wait(bar, phase);
-    phase ^= 1u;
-    const bool all = __syncthreads_and(done) != 0;
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    return all;
-}
-
-// 64 consecutive tensor-memory columns of this warp's lane quadrant: one
+// 32 consecutive tensor-memory columns of this warp's lane quadrant: one
 // load, one wait (a wait per 16 columns left the warps idle on its latency).
-__device__ __forceinline__ void tmem_ld64(uint32_t addr, float (&v)[64]) {
-    uint32_t r[64];
+__device__ __forceinline__ void tmem_ld(uint32_t addr, float (&v)[32]) {
+    uint32_t r[32];
     asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x64.b32 "
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
         "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,"
-        "%32,%33,%34,%35,%36,%37,%38,%39,%40,%41,%42,%43,%44,%45,%46,%47,"
-        "%48,%49,%50,%51,%52,%53,%54,%55,%56,%57,%58,%59,%60,%61,%62,%63}, [%64];\n"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
           "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
           "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31]),
-          "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]),
-          "=r"(r[40]), "=r"(r[41]), "=r"(r[42]), "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47]),
-          "=r"(r[48]), "=r"(r[49]), "=r"(r[50]), "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]), "=r"(r[55]),
-          "=r"(r[56]), "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]), "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
         : "r"(addr));
     asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 #pragma unroll
-    for (int i = 0; i < 64; ++i) v[i] = __uint_as_float(r[i]);
+    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
-
 // Four complex values (eight consecutive K elements of one operand row),
 // split into hi and lo 16-bit parts: one 16-byte store each.
 template <int PREC>
@@ -194,35 +173,39 @@ __device__ __forceinline__ void put4(unsigned char* xhi, unsigned char* xlo, uin
 }
 
 // From a first-pass result D = F X in tensor memory (rows 2u + c, columns
-// n = b * 64 + j): the second pass's operand X'[b * 64 + u][2j + c] =
-// D(u; j, b) * exp(-2 pi i u j / 4096). Warp (quadrant q4, half hh) takes
-// outputs u = 16 q4 .. 16 q4 + 15 of column b = hh; a lane pair (re row,
-// im row) swaps halves so each lane holds complex values of 8 items.
+// n = 2j + b: item j of column b): the second pass's operand
+// X'[2u + b][2j + c] = D(u; j, b) * exp(-2 pi i u j / 4096). Warp (quadrant
+// q4, part hh) takes outputs u = 16 q4 .. 16 q4 + 15 and D columns kCW hh ..
+// kCW hh + kCW - 1 (items of both columns). A lane pair (re row, im row)
+// trades halves so the even lane holds the complex values of column b = 0's
+// items and the odd lane column b = 1's: the pair reads one twiddle
+// (tw[j * 64 + u] = exp(-2 pi i u j / 4096), a broadcast) and writes rows
+// 2u and 2u + 1 of one operand chunk (distinct shared-memory bank quads).
 template <int PREC>
-__device__ __forceinline__ void second_pass_operand(uint32_t dtm, const float2* root, unsigned char* xhi,
+__device__ __forceinline__ void second_pass_operand(uint32_t dtm, const float2* tw, unsigned char* xhi,
                                                     unsigned char* xlo, int q4, int hh, int lane) {
     const int u = 16 * q4 + (lane >> 1);
-    const bool odd = (lane & 1) != 0;
-    const int m = 64 * hh + u;
-    float v[64];
-    tmem_ld64(dtm + uint32_t(64 * hh), v);
+    const int odd = lane & 1;
+    float v[kCW];
+    tmem_ld(dtm + uint32_t(kCW * hh), v);
 #pragma unroll
-    for (int c16 = 0; c16 < 4; ++c16) {
+    for (int c16 = 0; c16 < kCW / 16; ++c16) {
         float2 z[8];
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
-            const float send = odd ? v[16 * c16 + i] : v[16 * c16 + i + 8];
+            // Column 16 c16 + 2i (b = 0) and + 2i + 1 (b = 1) of this row.
+            const float send = odd ? v[16 * c16 + 2 * i] : v[16 * c16 + 2 * i + 1];
             const float got = __shfl_xor_sync(0xffffffffu, send, 1);
-            z[i] = odd ? make_float2(got, v[16 * c16 + i + 8]) : make_float2(v[16 * c16 + i], got);
+            z[i] = odd ? make_float2(got, v[16 * c16 + 2 * i + 1]) : make_float2(v[16 * c16 + 2 * i], got);
         }
-        const int j0 = 16 * c16 + (odd ? 8 : 0);
+        const int j0 = (kCW * hh + 16 * c16) >> 1;  // items j0 .. j0 + 7
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
-            const float2 w = root[u * (j0 + i)];
+            const float2 w = tw[(j0 + i) * 64 + u];
             z[i] = make_float2(__fmaf_rn(z[i].x, w.x, -z[i].y * w.y), __fmaf_rn(z[i].x, w.y, z[i].y * w.x));
         }
-        put4<PREC>(xhi, xlo, kmaj(m, 2 * j0), z);
-        put4<PREC>(xhi, xlo, kmaj(m, 2 * j0 + 8), z + 4);
+        put4<PREC>(xhi, xlo, kmaj(2 * u + odd, 2 * j0), z);
+        put4<PREC>(xhi, xlo, kmaj(2 * u + odd, 2 * j0 + 8), z + 4);
     }
 }
 
@@ -239,6 +222,7 @@ __global__ void __launch_bounds__(kT, 1)
     extern __shared__ __align__(1024) unsigned char sm[];
     __shared__ __align__(8) uint64_t bars[2];
     __shared__ uint32_t tmem_slot;
+    __shared__ int stop;  // a wait for an MMA ran out (read after block barriers)
     if (nk <= 0) return;
     constexpr uint32_t kCols = PIPE ? 2 * kTmemCols : kTmemCols;
     const int tid = int(threadIdx.x), warp = tid >> 5, lane = tid & 31;
@@ -248,21 +232,22 @@ __global__ void __launch_bounds__(kT, 1)
     // Operand slot s: hi at (2 + 2s) * kOp, lo at (3 + 2s) * kOp.
     const auto xhi = [&](int sl) { return sm + kSmXhi + uint32_t(sl) * 2u * kOp; };
     const auto xlo = [&](int sl) { return sm + kSmXlo + uint32_t(sl) * 2u * kOp; };
-    float2* root = reinterpret_cast<float2*>(sm + (PIPE ? kSmRoot + 2 * kOp : kSmRoot));
+    float2* tw = reinterpret_cast<float2*>(sm + (PIPE ? kSmRoot + 2 * kOp : kSmRoot));
     const uint32_t a_fhi = smem_u32(fhi), a_flo = smem_u32(flo);
 
-    // root[a] = exp(-2 pi i a / 4096).
+    // Second-pass twiddles tw[j * 64 + u] = exp(-2 pi i u j / 4096).
     for (int a = tid; a < kH; a += kT) {
         float sn, cs;
-        sincospif(float(a) * (1.0f / 2048.0f), &sn, &cs);
-        root[a] = make_float2(cs, -sn);
+        sincospif(float((a >> 6) * (a & 63)) * (1.0f / 2048.0f), &sn, &cs);
+        tw[a] = make_float2(cs, -sn);
     }
-    __syncthreads();
     // F: row 2u (re of output u) holds (cos, sin) of 2 pi u t / 64 against
     // (re, im) of input t, row 2u + 1 (im) holds (-sin, cos); over 64.
     for (int e = tid; e < 128 * 64; e += kT) {
         const int r = e >> 6, t = e & 63, u = r >> 1;
-        const float2 w = root[((u * t) & 63) * 64];  // exp(-2 pi i u t / 64)
+        float sn, cs;
+        sincospif(float((u * t) & 63) * (1.0f / 32.0f), &sn, &cs);
+        const float2 w = make_float2(cs, -sn);  // exp(-2 pi i u t / 64)
         const float a0 = ((r & 1) ? w.y : w.x) * (1.0f / 64.0f);
         const float a1 = ((r & 1) ? w.x : -w.y) * (1.0f / 64.0f);
         uint32_t h, l;
@@ -271,6 +256,7 @@ __global__ void __launch_bounds__(kT, 1)
         *reinterpret_cast<uint32_t*>(flo + kmaj(r, 2 * t)) = l;
     }
     if (tid == 0) {
+        stop = 0;
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&bars[0])) : "memory");
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&bars[1])) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
@@ -293,27 +279,31 @@ __global__ void __launch_bounds__(kT, 1)
     bool ok = true;
 
     // One pass on slot sl: operand writes made visible to the tensor cores,
-    // D = A B^T issued by one thread (not waited for).
+    // D = A B^T issued by one thread (not waited for). False for every
+    // thread, and nothing issued, once a wait has run out anywhere.
     const auto issue = [&](int sl, uint32_t d, uint32_t a_hi, uint32_t a_lo, uint32_t b_hi, uint32_t b_lo) {
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         __syncthreads();
+        if (*reinterpret_cast<volatile int*>(&stop)) return false;
         if (tid == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             issue_pass<PREC>(d, a_hi, a_lo, b_hi, b_lo, &bars[sl]);
         }
         pending |= 1u << sl;
+        return true;
     };
-    // Waits (bounded) for slot sl's pass; false for every thread if it ran out.
+    // Waits (bounded) for slot sl's pass. A wait that runs out raises `stop`
+    // and the thread carries on (its values are not used: the next `issue`,
+    // or the end of the kernel, stops every thread after a block barrier).
     const auto wait = [&](int sl) {
-        const bool done = mbar_wait(&bars[sl], (phases >> sl) & 1u);
-        const bool all = __syncthreads_and(done) != 0;
-        if (all) {
+        if (mbar_wait(&bars[sl], (phases >> sl) & 1u)) {
             phases ^= 1u << sl;
             pending &= ~(1u << sl);
+        } else {
+            *reinterpret_cast<volatile int*>(&stop) = 1;
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        return all;
     };
     const auto sx = [&](int sl) { return smem_u32(xhi(sl)); };
     const auto sxl = [&](int sl) { return smem_u32(xlo(sl)); };
@@ -326,30 +316,32 @@ __global__ void __launch_bounds__(kT, 1)
 
     for (int k0 = int(blockIdx.x) * kB; k0 < M && ok; k0 += int(gridDim.x) * kB) {
         const size_t gbase = size_t(k0 / KB) * kH * KB + size_t(k0 % KB);
-        // Forward first pass operand: X[b * 64 + j][2t + c] = S[j + 64 t][b];
-        // this thread's 16 rows (j = tid % 64, t = 4q .. 4q + 3 for q =
-        // tid / 64 + 4 it) all requested before any is used.
+        // Forward first pass operand: X[2j + b][2t + c] = S[j + 64 t][b] (the
+        // two columns' items interleaved);
+        // this thread's rows (j = tid % 64, t = 4q .. 4q + 3 for q =
+        // tid / 64 + (kT / 64) it) all requested before any is used.
         {
+            constexpr int kIt = 1024 / kT;
             const int j = tid & 63;
-            float4 sv[16];
+            float4 sv[4 * kIt];
 #pragma unroll
-            for (int it = 0; it < 4; ++it)
+            for (int it = 0; it < kIt; ++it)
 #pragma unroll
                 for (int i = 0; i < 4; ++i) {
-                    const int t = 4 * ((tid >> 6) + 4 * it) + i;
+                    const int t = 4 * ((tid >> 6) + (kT / 64) * it) + i;
                     sv[4 * it + i] = __ldg(reinterpret_cast<const float4*>(S + gbase + size_t(j + 64 * t) * KB));
                 }
 #pragma unroll
-            for (int it = 0; it < 4; ++it) {
-                const int q = (tid >> 6) + 4 * it;
+            for (int it = 0; it < kIt; ++it) {
+                const int q = (tid >> 6) + (kT / 64) * it;
                 float2 z0[4], z1[4];
 #pragma unroll
                 for (int i = 0; i < 4; ++i) {
                     z0[i] = make_float2(sv[4 * it + i].x, sv[4 * it + i].y);
                     z1[i] = make_float2(sv[4 * it + i].z, sv[4 * it + i].w);
                 }
-                put4<PREC>(xhi(0), xlo(0), kmaj(j, 8 * q), z0);
-                put4<PREC>(xhi(0), xlo(0), kmaj(64 + j, 8 * q), z1);
+                put4<PREC>(xhi(0), xlo(0), kmaj(2 * j, 8 * q), z0);
+                put4<PREC>(xhi(0), xlo(0), kmaj(2 * j + 1, 8 * q), z1);
             }
         }
         // The next group's rows into L2 while this group's passes run (a
@@ -360,52 +352,63 @@ __global__ void __launch_bounds__(kT, 1)
                 const float2* ns = S + size_t(nxt / KB) * kH * KB + size_t(nxt % KB);
                 for (int r = 2 * tid; r < kH; r += 2 * kT)
                     asm volatile("prefetch.global.L2 [%0];" ::"l"(ns + size_t(r) * KB));
+                // and its two columns of every kernel spectrum (2049 floats each)
+                constexpr int kLines = (kHh + 31) / 32;
+                for (int q = tid; q < nk * 2 * kLines; q += kT) {
+                    const int kk = q / (2 * kLines), c = (q / kLines) & 1, l = q % kLines;
+                    const float* kp = khat + (size_t(kk) * size_t(M + 1) + size_t(nxt + c)) * kHh + size_t(32 * l);
+                    asm volatile("prefetch.global.L2 [%0];" ::"l"(kp));
+                }
             }
         }
-        issue(0, wcol(0), a_fhi, a_flo, sx(0), sxl(0));
-        if (!(ok = wait(0))) break;
-        second_pass_operand<PREC>(wcol(0) + quad, root, xhi(0), xlo(0), q4, hh, lane);
-        // Column spectrum C = X F^T: row b * 64 + j' (item j' of column b),
+        if (!(ok = issue(0, wcol(0), a_fhi, a_flo, sx(0), sxl(0)))) break;
+        wait(0);
+        second_pass_operand<PREC>(wcol(0) + quad, tw, xhi(0), xlo(0), q4, hh, lane);
+        // Column spectrum C = X F^T: row 2j' + b (item j' of column b),
         // columns 2u' + c: C at ky = j' + 64 u' (over 4096).
-        issue(0, spec, sx(0), sxl(0), a_fhi, a_flo);
-        if (!(ok = wait(0))) break;
+        if (!(ok = issue(0, spec, sx(0), sxl(0), a_fhi, a_flo))) break;
+        wait(0);
 
-        // This lane's item of the spectrum: row m = 32 q4 + lane.
-        const int b = q4 >> 1, j = 32 * (q4 & 1) + lane, m = 32 * q4 + lane;
+        // This lane's item of the spectrum: row m = 32 q4 + lane (item j of
+        // column b; the lane pair (b = 0, 1) holds the same item of both).
+        const int b = lane & 1, j = 16 * q4 + (lane >> 1), m = 32 * q4 + lane;
         const int kx = k0 + b;
         if (k0 == 0) {
+            // Every lane loads (the tensor-memory load is warp-wide); the
+            // lanes of column 0 store.
+            float v[kCW];
+            tmem_ld(spec + quad + uint32_t(kCW * hh), v);
             if (b == 0) {
-                float v[64];
-                tmem_ld64(spec + quad + uint32_t(64 * hh), v);
 #pragma unroll
-                for (int i = 0; i < 32; ++i) c0[size_t(j + 64 * (32 * hh + i)) * KB] = make_float2(v[2 * i], v[2 * i + 1]);
+                for (int i = 0; i < kCW / 2; ++i)
+                    c0[size_t(j + 64 * ((kCW / 2) * hh + i)) * KB] = make_float2(v[2 * i], v[2 * i + 1]);
             }
             __syncthreads();  // column 0's spectrum visible to the block
         }
         // Inverse first pass operand of kernel kk (conjugated) into slot sl:
-        // X[m][2u' + c] = conj(C * khat) * 2^24, u' = 32 hh .. 32 hh + 31;
-        // the 32 kernel values are requested first.
+        // X[m][2u' + c] = conj(C * khat) * 2^24, u' = (kCW / 2) hh + e for
+        // e < kCW / 2; the kernel values are requested first.
         const auto product = [&](int kk, int sl) {
             const float* kh = khat + size_t(kk) * size_t(M + 1) * kHh;
-            float kv[32];
+            float kv[kCW / 2];
 #pragma unroll
-            for (int i = 0; i < 32; ++i) {
-                const int ky = j + 64 * (32 * hh + i);
+            for (int i = 0; i < kCW / 2; ++i) {
+                const int ky = j + 64 * ((kCW / 2) * hh + i);
                 kv[i] = __ldg(kh + size_t(kx) * kHh + min(ky, kH - ky));
             }
-            float v[64];
-            tmem_ld64(spec + quad + uint32_t(64 * hh), v);
+            float v[kCW];
+            tmem_ld(spec + quad + uint32_t(kCW * hh), v);
 #pragma unroll
-            for (int c8 = 0; c8 < 4; ++c8) {
+            for (int c8 = 0; c8 < kCW / 16; ++c8) {
                 float2 z[8];
 #pragma unroll
                 for (int i = 0; i < 8; ++i) {
-                    const int e = 8 * c8 + i;  // u' = 32 hh + e
+                    const int e = 8 * c8 + i;  // u' = (kCW / 2) hh + e
                     const float P = kv[e] * kProductScale;
                     if (kx == 0) {
                         // Packed column 0: X[0] and X[M] (both real) as re/im;
                         // the product splits them with C[ky] and conj C[-ky].
-                        const int ky = j + 64 * (32 * hh + e);
+                        const int ky = j + 64 * ((kCW / 2) * hh + e);
                         const float Q = __ldg(kh + size_t(M) * kHh + min(ky, kH - ky)) * kProductScale;
                         const float2 cm = c0[size_t(ky == 0 ? 0 : kH - ky) * KB];
                         const float ev = 0.5f * (P + Q), od = 0.5f * (P - Q);
@@ -414,54 +417,70 @@ __global__ void __launch_bounds__(kT, 1)
                         z[i] = make_float2(v[2 * e] * P, -v[2 * e + 1] * P);
                     }
                 }
-                const int kc = 64 * hh + 16 * c8;
+                const int kc = kCW * hh + 16 * c8;
                 put4<PREC>(xhi(sl), xlo(sl), kmaj(m, kc), z);
                 put4<PREC>(xhi(sl), xlo(sl), kmaj(m, kc + 8), z + 4);
             }
         };
         // U_kk = conj(D) from slot sl: row m = item j of column b, columns
-        // 2u' + c at ky = j + 64 u'.
+        // 2u' + c at ky = j + 64 u'. The lane pair swaps halves so each lane
+        // writes both columns of a row (16 bytes, the group's whole share of
+        // a block row): lane b = 0 the first half of its outputs u', lane
+        // b = 1 the second.
         const auto output = [&](int kk, int sl) {
-            float2* dst = U + size_t(kk) * size_t(M) * kH + gbase + b;
-            float v[64];
-            tmem_ld64(wcol(sl) + quad + uint32_t(64 * hh), v);
+            float2* dst = U + size_t(kk) * size_t(M) * kH + gbase;
+            float v[kCW];
+            tmem_ld(wcol(sl) + quad + uint32_t(kCW * hh), v);
+            constexpr int kH4 = kCW / 4;  // outputs per lane after the swap
 #pragma unroll
-            for (int i = 0; i < 32; ++i) dst[size_t(j + 64 * (32 * hh + i)) * KB] = make_float2(v[2 * i], -v[2 * i + 1]);
+            for (int i = 0; i < kH4; ++i) {
+                const float sr = b ? v[2 * i] : v[2 * (kH4 + i)], si = b ? v[2 * i + 1] : v[2 * (kH4 + i) + 1];
+                const float gr = __shfl_xor_sync(0xffffffffu, sr, 1), gi = __shfl_xor_sync(0xffffffffu, si, 1);
+                const int e = b ? kH4 + i : i;  // u' = (kCW / 2) hh + e
+                const float4 q = b ? make_float4(gr, -gi, v[2 * e], -v[2 * e + 1])
+                                   : make_float4(v[2 * e], -v[2 * e + 1], gr, -gi);
+                *reinterpret_cast<float4*>(dst + size_t(j + 64 * ((kCW / 2) * hh + e)) * KB) = q;
+            }
         };
         // Inverse transforms of kernel kk on slot sl: first pass issued by
         // `first`, the second pass's operand built and issued by `second`.
         const auto first = [&](int kk, int sl) {
             product(kk, sl);
-            issue(sl, wcol(sl), a_fhi, a_flo, sx(sl), sxl(sl));
+            return issue(sl, wcol(sl), a_fhi, a_flo, sx(sl), sxl(sl));
         };
         const auto second = [&](int sl) {
-            second_pass_operand<PREC>(wcol(sl) + quad, root, xhi(sl), xlo(sl), q4, hh, lane);
-            issue(sl, wcol(sl), sx(sl), sxl(sl), a_fhi, a_flo);
+            second_pass_operand<PREC>(wcol(sl) + quad, tw, xhi(sl), xlo(sl), q4, hh, lane);
+            return issue(sl, wcol(sl), sx(sl), sxl(sl), a_fhi, a_flo);
         };
         if constexpr (!PIPE) {
             for (int kk = 0; kk < nk; ++kk) {
-                first(kk, 0);
-                if (!(ok = wait(0))) break;
-                second(0);
-                if (!(ok = wait(0))) break;
+                if (!(ok = first(kk, 0))) break;
+                wait(0);
+                if (!(ok = second(0))) break;
+                wait(0);
                 output(kk, 0);
             }
         } else {
-            first(0, 0);
-            if (nk > 1) first(1, 1);
+            if (!(ok = first(0, 0))) break;
+            if (nk > 1 && !(ok = first(1, 1))) break;
             for (int k = 0; k < nk; ++k) {
                 const int sl = k & 1;
-                if (!(ok = wait(sl))) break;  // kernel k's first pass
-                second(sl);
+                wait(sl);  // kernel k's first pass
+                if (!(ok = second(sl))) break;
                 if (k >= 1) {
-                    if (!(ok = wait(sl ^ 1))) break;  // kernel k - 1's second pass
+                    wait(sl ^ 1);  // kernel k - 1's second pass
                     output(k - 1, sl ^ 1);
-                    if (k + 1 < nk) first(k + 1, sl ^ 1);
+                    if (k + 1 < nk && !(ok = first(k + 1, sl ^ 1))) break;
                 }
             }
-            if (ok && (ok = wait((nk - 1) & 1))) output(nk - 1, (nk - 1) & 1);
+            if (ok) {
+                wait((nk - 1) & 1);
+                output(nk - 1, (nk - 1) & 1);
+            }
         }
     }
+    __syncthreads();
+    if (*reinterpret_cast<volatile int*>(&stop)) ok = false;
     if (!ok) {
         // A wait ran out: count it once per CTA and give the MMAs still in
         // flight one more bounded wait before the tensor memory is freed.
