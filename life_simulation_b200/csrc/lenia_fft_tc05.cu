@@ -334,14 +334,19 @@ __global__ void __launch_bounds__(kT, 1)
 #pragma unroll
             for (int it = 0; it < kIt; ++it) {
                 const int q = (tid >> 6) + (kT / 64) * it;
+                // Rows 2j (column 0) and 2j + 1 (column 1); lanes with j % 8 >= 4
+                // write the odd row first, so each store's eight-lane phase
+                // covers eight distinct bank quads.
+                const int sw = (j >> 2) & 1;
                 float2 z0[4], z1[4];
 #pragma unroll
                 for (int i = 0; i < 4; ++i) {
-                    z0[i] = make_float2(sv[4 * it + i].x, sv[4 * it + i].y);
-                    z1[i] = make_float2(sv[4 * it + i].z, sv[4 * it + i].w);
+                    const float4 a = sv[4 * it + i];
+                    z0[i] = sw ? make_float2(a.z, a.w) : make_float2(a.x, a.y);
+                    z1[i] = sw ? make_float2(a.x, a.y) : make_float2(a.z, a.w);
                 }
-                put4<PREC>(xhi(0), xlo(0), kmaj(2 * j, 8 * q), z0);
-                put4<PREC>(xhi(0), xlo(0), kmaj(2 * j + 1, 8 * q), z1);
+                put4<PREC>(xhi(0), xlo(0), kmaj(2 * j + sw, 8 * q), z0);
+                put4<PREC>(xhi(0), xlo(0), kmaj(2 * j + 1 - sw, 8 * q), z1);
             }
         }
         // The next group's rows into L2 while this group's passes run (a
