@@ -171,3 +171,34 @@ def test_tcgen05_engine_equals_fp32_path_closely():
         m.close()
     d = np.abs(fields["fp16x3"] - fields["fp32"]).max()
     assert d <= 1e-3, d
+
+
+@pytest.mark.parametrize("engine", ["tcgen05_serial", "tcgen05_pipelined"])
+@pytest.mark.parametrize("nk,width", [(1, 512), (2, 1024), (4, 4096)])
+def test_tcgen05_kernel_counts_and_widths(engine, nk, width):
+    """The tcgen05 pass with 1, 2 and 4 kernels (the pipelined schedule's
+    one-, two- and four-kernel paths) on 4096-row fields of 512, 1024 and
+    4096 columns (128, 256 and 1024 column groups: fewer than the CTAs, an
+    uneven number per CTA, seven per CTA): per-step error against FP64."""
+    w, h = width, 4096
+    params = tc_params(w, h, "fp16x3", radius=24)
+    ks = wl.fft3_params(w, h)["kernels"]
+    if nk == 4:
+        extra = dict(ks[0])
+        extra["mu"], extra["weight"] = 0.21, 0.25
+        ks = ks + [extra]
+    params["kernels"] = ks[:nk]
+    m = tc_module(params, w, h, engine)
+    info = m.info()
+    assert info["tc_engine"] == TC05_ENGINE[engine] and info["num_kernels"] == nk, info
+    m.close()
+    import os
+
+    init = wl.patches(w, h, 12, 128, seed=9)
+    os.environ["LENIA_TC_ENGINE"] = engine
+    try:
+        errs = step_errors(params, w, h, init, 2)
+    finally:
+        os.environ.pop("LENIA_TC_ENGINE", None)
+    print(f"{w}x{h} K={nk} {engine}: per-step max {errs[:, 0].max():.2e}")
+    assert errs[:, 0].max() <= TOL["fp16x3"], errs
